@@ -1,0 +1,160 @@
+/*
+ * stratiflow_b200 — C-ABI of the B200 IMEX-RK time-step engine.
+ *
+ * The reference (jeremypparker/Stratiflow) has no FFI: its hot path is the
+ * C++ class IMEXRK (IMEXRK.h:31-670), held as the static StateVector::solver
+ * (StateVector.h:546) and driven by StateVector::FullEvolve / FixedEvolve /
+ * LinearEvolve (StateVector.cpp:3-156). Each entry point below replaces one
+ * member of that surface; the comment on each names the member it replaces.
+ *
+ * Conventions
+ *   - Every function returns 0 on success and a negative SF_E* code on
+ *     failure; sf_last_error() then returns a message (thread-local). No C++
+ *     exception crosses this boundary.
+ *   - A solver owns one CUDA stream on one device and all its device memory.
+ *     Calls on one solver must come from one host thread at a time.
+ *   - Grid sizes are runtime values (the reference fixes them at compile time,
+ *     Parameters.h:42-43). N1 and N2 are powers of two, 16 <= N1 <= 512,
+ *     N2 == 1 (2D) or 16 <= N2 <= 256 (3D); N3 % 4 == 0, 16 <= N3 <= 1024.
+ *   - A solver advances `nrun` independent runs of the same grid together
+ *     (ensemble members, Krylov directions); each run has its own Ri,
+ *     background profile and state.
+ *   - Field data in the reference layout is std::complex<float> interleaved,
+ *     z fastest: index (M1*n2 + n1)*N3 + n3 with M1 = N1/2+1 (Field.h:399,410),
+ *     i.e. exactly ModalField::Raw(). Only the kept (2/3-dealiased) modes are
+ *     stored on the device; set_field ignores the others and get_field writes
+ *     them as zero (the state the reference's FilterAll leaves them in).
+ *   - The compact device layout ("kept layout") is complex<float>
+ *     [N3][plane], plane = roundup(K1*K2, 16), mode index m = q*K1 + j1,
+ *     K1 = N1/3 x-modes, K2 = 1 (2D) or 2*(N2/3)-1 y-modes in the order
+ *     ky = 0..N2/3-1, -(N2/3-1)..-1.
+ */
+#ifndef STRATIFLOW_B200_H
+#define STRATIFLOW_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SF_OK 0
+#define SF_EINVAL (-1)   /* bad argument or grid */
+#define SF_ECUDA (-2)    /* CUDA runtime error */
+#define SF_ENOMEM (-3)   /* device allocation failed */
+#define SF_ESTATE (-4)   /* call out of order (e.g. linear step without base) */
+
+/* field selectors: IMEXRK public members u1,u2,u3,b,p (IMEXRK.h:605-606) */
+#define SF_U1 0
+#define SF_U2 1
+#define SF_U3 2
+#define SF_B 3
+#define SF_P 4
+
+typedef struct sf_solver sf_solver;
+
+/* gridParams (Parameters.h:6-18, 42-43) plus the batch size */
+typedef struct {
+  int N1, N2, N3;
+  int nrun;
+} sf_grid;
+
+/* flowParams (Parameters.h:20-30, Parameters.cpp:5-6); Ri is set per run */
+typedef struct {
+  double L1, L2, L3, Re, Pr;
+} sf_flow;
+
+/* IMEXRK::IMEXRK (IMEXRK.h:37-81): builds the Laplacian factors and, via
+ * UpdateForTimestep, the Crank-Nicolson factors for deltaT = dt. All runs
+ * start with Ri = 0, a zero background and a zero state. */
+int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, sf_solver** out);
+
+/* releases the device memory, graphs and stream */
+int sf_destroy(sf_solver* s);
+
+/* message of the last failing call on this host thread */
+const char* sf_last_error(void);
+
+/* IMEXRK::deltaT + UpdateForTimestep (IMEXRK.h:502-545): re-factorises the
+ * tridiagonal systems in FP64 on the device */
+int sf_set_dt(sf_solver* s, double dt);
+
+/* flowParams.Ri for one run (enters BuildRHS only, IMEXRK.cpp:143) */
+int sf_set_ri(sf_solver* s, int run, double Ri);
+
+/* IMEXRK::SetBackground(Neumann1D) (IMEXRK.h:321-332): U_[N3] at the
+ * Neumann levels, plus the background stratification dB/dz[N3] at the same
+ * levels, which generalises the dB/dz = 1 hard-wired in BuildRHS
+ * (IMEXRK.cpp:145-147; pass all ones for the reference's behaviour). */
+int sf_set_background(sf_solver* s, int run, const double* U, const double* dBdz);
+
+/* assignment to solver.u1/u2/u3/b/p (StateVector::CopyToSolver,
+ * StateVector.h:511-525) from host memory in the reference layout */
+int sf_set_field(sf_solver* s, int run, int field, const float* ref_layout);
+
+/* StateVector::CopyFromSolver (StateVector.h:532-543) into host memory in
+ * the reference layout */
+int sf_get_field(sf_solver* s, int run, int field, float* ref_layout);
+
+/* whole state (u1,u2,u3,b,p) of every run, host <-> device, in the kept
+ * layout, one contiguous buffer [nrun][5][N3][plane] of complex<float> */
+int sf_set_state_kept(sf_solver* s, const float* host);
+int sf_get_state_kept(sf_solver* s, float* host);
+
+/* device pointer of the current state in the kept layout (valid until the
+ * next step call), and its size in bytes */
+int sf_state_device(sf_solver* s, void** dptr, size_t* bytes);
+/* copy a device buffer in the kept layout into the current state */
+int sf_set_state_device(sf_solver* s, const void* dptr);
+
+/* StateVector::FixedEvolve's set-up (StateVector.cpp:94-97): FilterAll,
+ * PopulateNodalVariables, RemoveDivergence(0) for every run */
+int sf_prepare(sf_solver* s);
+
+/* IMEXRK::RemoveDivergence(pressureMultiplier) (IMEXRK.cpp:43-73) */
+int sf_remove_divergence(sf_solver* s, double pressure_multiplier);
+
+/* nsteps x IMEXRK::TimeStep (IMEXRK.cpp:8-24) for every run; replays a
+ * captured CUDA graph of one step; asynchronous on the solver's stream */
+int sf_step(sf_solver* s, int nsteps);
+
+/* IMEXRK::SetBackground(u1,u2,u3,b) (IMEXRK.h:334-352): the frozen base state
+ * of TimeStepLinear for one run, modal, reference layout */
+int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const float* u3,
+                const float* b);
+
+/* nsteps x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41) */
+int sf_step_linear(sf_solver* s, int nsteps);
+
+/* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
+int sf_energy(sf_solver* s, int run, double* ke, double* pe);
+
+/* StateVector::Dot (StateVector.h:122-134) between run a of solver sa and
+ * run b of solver sb (same grid), FP64 accumulation; Ri of run a weights b */
+int sf_dot(sf_solver* sa, int run_a, sf_solver* sb, int run_b, double* out);
+
+/* Per-kernel timing of one step (no counterpart in the reference, which has
+ * no timers): runs nsteps steps eagerly (not from the graph) with CUDA events
+ * between kernel launches and writes the average milliseconds of each kernel
+ * slot of one step into ms[0..*nslots); the state advances as by sf_step /
+ * sf_step_linear (linear != 0). Slot order is that of sf_profile_names. */
+int sf_profile_step(sf_solver* s, int nsteps, int linear, int cap, double* ms, int* nslots);
+
+/* comma-separated kernel names of the profile slots */
+int sf_profile_names(sf_solver* s, char* buf, size_t len);
+
+/* waits for all work queued on the solver's stream */
+int sf_synchronize(sf_solver* s);
+
+/* the solver's stream (cudaStream_t) for callers that order their own work */
+int sf_stream(sf_solver* s, void** stream);
+
+/* number of this library's kernel launches issued so far by the solver */
+int sf_launch_count(sf_solver* s, long long* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STRATIFLOW_B200_H */

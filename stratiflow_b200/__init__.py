@@ -1,0 +1,263 @@
+"""stratiflow_b200 — B200-native IMEX-RK time step of a stratified shear flow.
+
+Python front end over the C-ABI in ``include/stratiflow_b200.h``. The
+solver object mirrors the reference's ``IMEXRK`` (IMEXRK.h:31-670): the same
+operations under the same names, on a batch of runs held on one GPU.
+
+The CUDA library must have been built (``python -m stratiflow_b200.build``);
+there is no CPU fallback: importing this package without it raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .grid import (background_profile, kept_modes, neumann_profile, vertical_points,
+                   vertical_points_fractional)
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libstratiflow_b200.so")
+
+U1, U2, U3, B, P = 0, 1, 2, 3, 4
+FIELD = {"u1": U1, "u2": U2, "u3": U3, "b": B, "p": P}
+
+# every entry point declared in include/stratiflow_b200.h
+EXPORTS = [
+    "sf_create", "sf_destroy", "sf_last_error", "sf_set_dt", "sf_set_ri", "sf_set_background",
+    "sf_set_field", "sf_get_field", "sf_set_state_kept", "sf_get_state_kept", "sf_state_device",
+    "sf_set_state_device", "sf_prepare", "sf_remove_divergence", "sf_step", "sf_set_base",
+    "sf_step_linear", "sf_energy", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
+    "sf_profile_step", "sf_profile_names",
+]
+
+
+class SFError(RuntimeError):
+    pass
+
+
+class _Grid(C.Structure):
+    _fields_ = [("N1", C.c_int), ("N2", C.c_int), ("N3", C.c_int), ("nrun", C.c_int)]
+
+
+class _Flow(C.Structure):
+    _fields_ = [("L1", C.c_double), ("L2", C.c_double), ("L3", C.c_double), ("Re", C.c_double),
+                ("Pr", C.c_double)]
+
+
+_lib = None
+
+
+def load_library(path: str | None = None):
+    """Load ``libstratiflow_b200.so``; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise SFError(f"{path} is missing: build it with `python -m stratiflow_b200.build`")
+    L = C.CDLL(path)
+    vp, i, d = C.c_void_p, C.c_int, C.c_double
+    dp, fp = C.POINTER(C.c_double), C.c_void_p
+    sig = {
+        "sf_create": [C.POINTER(_Grid), C.POINTER(_Flow), d, i, C.POINTER(vp)],
+        "sf_destroy": [vp], "sf_set_dt": [vp, d], "sf_set_ri": [vp, i, d],
+        "sf_set_background": [vp, i, dp, dp], "sf_set_field": [vp, i, i, fp],
+        "sf_get_field": [vp, i, i, fp], "sf_set_state_kept": [vp, fp], "sf_get_state_kept": [vp, fp],
+        "sf_state_device": [vp, C.POINTER(vp), C.POINTER(C.c_size_t)], "sf_set_state_device": [vp, vp],
+        "sf_prepare": [vp], "sf_remove_divergence": [vp, d], "sf_step": [vp, i],
+        "sf_set_base": [vp, i, fp, fp, fp, fp], "sf_step_linear": [vp, i],
+        "sf_energy": [vp, i, dp, dp], "sf_dot": [vp, i, vp, i, dp], "sf_synchronize": [vp],
+        "sf_stream": [vp, C.POINTER(vp)], "sf_launch_count": [vp, C.POINTER(C.c_longlong)],
+        "sf_profile_step": [vp, i, i, i, dp, C.POINTER(i)], "sf_profile_names": [vp, C.c_char_p, C.c_size_t],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = C.c_int
+    L.sf_last_error.argtypes = []
+    L.sf_last_error.restype = C.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != 0:
+        msg = load_library().sf_last_error().decode(errors="replace")
+        raise SFError(f"stratiflow_b200 error {rc}: {msg}")
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class IMEXRK:
+    """A batch of ``nrun`` independent IMEX-RK integrations of one grid on one
+    GPU; the device-resident counterpart of the reference's ``IMEXRK``
+    (IMEXRK.h:31-670) with runtime grid sizes (Parameters.h:42-43)."""
+
+    def __init__(self, N1, N2, N3, L1, L2, L3, Re, Pr, dt, nrun=1, device=0):
+        L = load_library()
+        self.N1, self.N2, self.N3, self.nrun = int(N1), int(N2), int(N3), int(nrun)
+        self.M1 = self.N1 // 2 + 1
+        self.L1, self.L2, self.L3, self.Re, self.Pr = float(L1), float(L2), float(L3), float(Re), float(Pr)
+        self.deltaT = float(dt)
+        g = _Grid(self.N1, self.N2, self.N3, self.nrun)
+        f = _Flow(self.L1, self.L2, self.L3, self.Re, self.Pr)
+        h = C.c_void_p()
+        _check(L.sf_create(C.byref(g), C.byref(f), self.deltaT, int(device), C.byref(h)))
+        self._h = h
+        self.dim3 = self.N2 > 1
+        self.K1 = self.N1 // 3
+        self.K2 = 2 * (self.N2 // 3) - 1 if self.dim3 else 1
+        self.plane = (self.K1 * self.K2 + 15) // 16 * 16
+        self.Ri = np.zeros(self.nrun)
+
+    # ---- lifetime ----
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().sf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- parameters ----
+    def UpdateForTimestep(self, dt=None):
+        """deltaT assignment + UpdateForTimestep (IMEXRK.h:502-545)."""
+        if dt is not None:
+            self.deltaT = float(dt)
+        _check(load_library().sf_set_dt(self._h, self.deltaT))
+
+    def set_ri(self, run, Ri):
+        self.Ri[run] = float(Ri)
+        _check(load_library().sf_set_ri(self._h, int(run), float(Ri)))
+
+    def SetBackground(self, run, U, dBdz=None):
+        """IMEXRK::SetBackground(Neumann1D) (IMEXRK.h:321-332) plus the
+        background stratification profile (ones = the reference)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        dB = np.ones(self.N3) if dBdz is None else np.ascontiguousarray(dBdz, dtype=np.float64)
+        _check(load_library().sf_set_background(self._h, int(run), U.ctypes.data_as(C.POINTER(C.c_double)),
+                                                dB.ctypes.data_as(C.POINTER(C.c_double))))
+
+    # ---- fields (reference layout [N2][M1][N3] complex64) ----
+    @property
+    def modal_shape(self):
+        return (self.N2, self.M1, self.N3)
+
+    def set_field(self, run, name, arr):
+        a = np.ascontiguousarray(np.asarray(arr).reshape(self.modal_shape), dtype=np.complex64)
+        _check(load_library().sf_set_field(self._h, int(run), FIELD[name], _fptr(a)))
+
+    def get_field(self, run, name):
+        out = np.zeros(self.modal_shape, dtype=np.complex64)
+        _check(load_library().sf_get_field(self._h, int(run), FIELD[name], _fptr(out)))
+        return out
+
+    def set_state(self, run, st: dict):
+        for k, v in st.items():
+            self.set_field(run, k, v)
+
+    def get_state(self, run, names=("u1", "u2", "u3", "b", "p")):
+        return {k: self.get_field(run, k) for k in names}
+
+    # ---- kept layout, all runs at once ----
+    @property
+    def kept_shape(self):
+        return (self.nrun, 5, self.N3, self.plane)
+
+    def set_state_kept(self, a):
+        a = np.ascontiguousarray(a, dtype=np.complex64).reshape(self.kept_shape)
+        _check(load_library().sf_set_state_kept(self._h, _fptr(a)))
+
+    def get_state_kept(self, out=None):
+        if out is None:
+            out = np.zeros(self.kept_shape, dtype=np.complex64)
+        _check(load_library().sf_get_state_kept(self._h, _fptr(out)))
+        return out
+
+    def state_device_ptr(self):
+        p, n = C.c_void_p(), C.c_size_t()
+        _check(load_library().sf_state_device(self._h, C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+    def set_state_device(self, ptr):
+        _check(load_library().sf_set_state_device(self._h, C.c_void_p(ptr)))
+
+    # ---- the scheme ----
+    def Prepare(self):
+        """FilterAll + RemoveDivergence(0) (StateVector.cpp:94-97)."""
+        _check(load_library().sf_prepare(self._h))
+
+    def RemoveDivergence(self, pressure_multiplier=1.0):
+        _check(load_library().sf_remove_divergence(self._h, float(pressure_multiplier)))
+
+    def TimeStep(self, n=1):
+        """n x IMEXRK::TimeStep (IMEXRK.cpp:8-24) on every run; asynchronous."""
+        _check(load_library().sf_step(self._h, int(n)))
+
+    def SetBase(self, run, u1, u2, u3, b):
+        """IMEXRK::SetBackground(u1,u2,u3,b) (IMEXRK.h:334-352)."""
+        arrs = [np.ascontiguousarray(np.asarray(x).reshape(self.modal_shape), dtype=np.complex64)
+                for x in (u1, u2, u3, b)]
+        _check(load_library().sf_set_base(self._h, int(run), *[_fptr(x) for x in arrs]))
+
+    def TimeStepLinear(self, n=1):
+        """n x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41); asynchronous."""
+        _check(load_library().sf_step_linear(self._h, int(n)))
+
+    def energy(self, run=0):
+        """(KE, PE) of one run (IMEXRK.h:395-411), FP64 accumulation."""
+        ke, pe = C.c_double(), C.c_double()
+        _check(load_library().sf_energy(self._h, int(run), C.byref(ke), C.byref(pe)))
+        return ke.value, pe.value
+
+    def KE(self, run=0):
+        return self.energy(run)[0]
+
+    def PE(self, run=0):
+        return self.energy(run)[1]
+
+    def dot(self, run_a, other: "IMEXRK", run_b):
+        out = C.c_double()
+        _check(load_library().sf_dot(self._h, int(run_a), other._h, int(run_b), C.byref(out)))
+        return out.value
+
+    def synchronize(self):
+        _check(load_library().sf_synchronize(self._h))
+
+    def stream(self):
+        p = C.c_void_p()
+        _check(load_library().sf_stream(self._h, C.byref(p)))
+        return p.value
+
+    def profile_step(self, nsteps=3, linear=False):
+        """{kernel slot name: average ms} of one step, timed eagerly with
+        CUDA events between launches; advances the state by nsteps steps."""
+        L = load_library()
+        cap = 64
+        ms = (C.c_double * cap)()
+        n = C.c_int()
+        _check(L.sf_profile_step(self._h, int(nsteps), int(bool(linear)), cap, ms, C.byref(n)))
+        buf = C.create_string_buffer(4096)
+        _check(L.sf_profile_names(self._h, buf, 4096))
+        names = buf.value.decode().split(",")
+        return [(f"s{i // (n.value // 3)}:{names[i]}", ms[i]) for i in range(n.value)]
+
+    def launch_count(self):
+        n = C.c_longlong()
+        _check(load_library().sf_launch_count(self._h, C.byref(n)))
+        return n.value
+
+
+__all__ = ["IMEXRK", "SFError", "load_library", "EXPORTS", "vertical_points",
+           "vertical_points_fractional", "neumann_profile", "background_profile", "kept_modes"]

@@ -1,0 +1,860 @@
+// CUDA kernels of one IMEX-RK stage (IMEXRK.cpp:8-24 / 26-41) for sm_100a.
+//
+// A stage runs as
+//   [3D] k_ifft_y   modal u1,u2,u3,b -> (kx, y) rows          (ModalField::ToNodal, y part)
+//        k_xpass    per (y row, slab of z levels): c2r along x, the nodal
+//                   products of BuildRHS / BuildRHSLinear, r2c along x,
+//                   1/(N1 N2), 2/3 truncation and the z stencils and
+//                   x-derivatives that follow each product
+//   [3D] k_fft_y    (kx, y) -> (kx, ky), y-derivatives, sum into r
+//        k_z_cn     per (mode, field): ExplicitRK + linear buoyancy terms +
+//                   FinishRHS + CrankNicolson right-hand side + Thomas solve
+//        k_z_proj   per mode: divergence, Laplacian solve, projection, p update
+// Every kernel touches only kept (dealiased) modes, which is all the reference's
+// ModalField arithmetic touches (Field.h:1129-1166).
+
+#include "sf_internal.cuh"
+
+namespace sf {
+
+// ===================================================== y transforms (3D) ====
+constexpr int kCG = 16;          // kx columns per block in the y transforms
+constexpr int kYThreads = 128;
+
+__device__ __forceinline__ int n2_of_q(int q, int Ky, int K2, int N2) { return q < Ky ? q : q + N2 - K2; }
+
+// modal [q][j1] of (run, field f, level j) -> mixed [y][j1], inverse c2c in y
+__global__ void __launch_bounds__(kYThreads) k_ifft_y(StageArgs a) {
+  const Geo g = a.g;
+  extern __shared__ float2 smem[];
+  const int ld = g.N2 + 1;
+  const int cg0 = blockIdx.x * kCG;
+  const int j = blockIdx.y;
+  const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
+  const float2* src = a.S + ((size_t)(run * 5 + f) * g.N3 + j) * g.Pp;
+  for (int i = threadIdx.x; i < kCG * ld; i += blockDim.x) smem[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  for (int i = threadIdx.x; i < g.K2 * kCG; i += blockDim.x) {
+    int q = i / kCG, c = i - q * kCG, j1 = cg0 + c;
+    if (j1 < g.K1) smem[c * ld + n2_of_q(q, g.Ky, g.K2, g.N2)] = src[q * g.K1 + j1];
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int c = warp; c < kCG; c += nw)
+    if (cg0 + c < g.K1) warp_fft(smem + c * ld, g.N2, g.logN2, a.tw, true, lane);
+  __syncthreads();
+  float2* dst = a.mixin + ((size_t)(run * 4 + f) * g.N3 + j) * g.N2 * g.K1;
+  for (int i = threadIdx.x; i < g.N2 * kCG; i += blockDim.x) {
+    int y = i / kCG, c = i - y * kCG, j1 = cg0 + c;
+    if (j1 < g.K1) dst[(size_t)y * g.K1 + j1] = smem[c * ld + y];
+  }
+}
+
+// mixed combos (C_f, C_fy) [y][j1] -> r_f[q][j1] = Fy(C_f) + i ky Fy(C_fy)
+__global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
+  const Geo g = a.g;
+  extern __shared__ float2 smem[];
+  const int ld = g.N2 + 1;
+  const int cg0 = blockIdx.x * kCG;
+  const int j = blockIdx.y;
+  const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
+  const float2* cA = a.mixout + ((size_t)(run * 8 + 2 * f) * g.N3 + j) * g.N2 * g.K1;
+  const float2* cB = a.mixout + ((size_t)(run * 8 + 2 * f + 1) * g.N3 + j) * g.N2 * g.K1;
+  for (int i = threadIdx.x; i < g.N2 * kCG; i += blockDim.x) {
+    int y = i / kCG, c = i - y * kCG, j1 = cg0 + c;
+    float2 va = make_float2(0.f, 0.f), vb = va;
+    if (j1 < g.K1) {
+      va = cA[(size_t)y * g.K1 + j1];
+      vb = cB[(size_t)y * g.K1 + j1];
+    }
+    smem[c * ld + y] = va;
+    smem[(kCG + c) * ld + y] = vb;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int c = warp; c < 2 * kCG; c += nw)
+    if (cg0 + (c % kCG) < g.K1) warp_fft(smem + c * ld, g.N2, g.logN2, a.tw, false, lane);
+  __syncthreads();
+  float2* dst = a.rnl + ((size_t)(run * 4 + f) * g.N3 + j) * g.Pp;
+  for (int i = threadIdx.x; i < g.K2 * kCG; i += blockDim.x) {
+    int q = i / kCG, c = i - q * kCG, j1 = cg0 + c;
+    if (j1 < g.K1) {
+      int n2 = n2_of_q(q, g.Ky, g.K2, g.N2);
+      float2 v = cadd(smem[c * ld + n2], cik(a.ky[q], smem[(kCG + c) * ld + n2]));
+      dst[q * g.K1 + j1] = v;
+    }
+  }
+}
+
+// ============================================================= x pass ====
+// product ids (BuildRHS, IMEXRK.cpp:155-192; BuildRHSLinear, :212-257)
+enum Prod { P_S1, P_SB1, P_P3, P_Q1, P_QB, P_P4, P_S12, P_S22, P_SB2, P_Q2, P_P3Y, P_COUNT };
+
+constexpr int kXThreads = 256;
+constexpr int kXWarps = kXThreads / 32;
+
+struct XLayout {  // shared-memory carve-up of k_xpass
+  int S, N1, K1, nprod;
+  size_t hat_off, work_off, nod_off, base_off, bytes;
+};
+
+__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear) {
+  XLayout L;
+  L.S = S; L.N1 = N1; L.K1 = K1;
+  L.nprod = dim3 ? P_COUNT : 6;
+  size_t off = 0;
+  L.hat_off = off;  off += sizeof(float2) * (size_t)L.nprod * (S + 2) * K1;
+  L.work_off = off; off += sizeof(float2) * (size_t)kXWarps * N1;
+  L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
+  L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
+  L.bytes = off;
+  return L;
+}
+
+// slots s = 0..S+1 hold level j0-1+s; product p is formed at slots
+// [first, first+count)
+__device__ __forceinline__ void prod_slots(int p, int S, int& first, int& count) {
+  if (p == P_Q1 || p == P_QB || p == P_Q2) { first = 1; count = S + 1; }
+  else if (p == P_P4) { first = 0; count = S + 1; }
+  else { first = 1; count = S; }
+}
+
+template <int S, bool LINEAR>
+__global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a) {
+  const Geo g = a.g;
+  extern __shared__ __align__(16) unsigned char xsm[];
+  const XLayout L = x_layout(S, g.N1, g.K1, g.dim3, LINEAR);
+  float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
+  float2* work = reinterpret_cast<float2*>(xsm + L.work_off);
+  float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
+  float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
+  const int N1 = g.N1, K1 = g.K1, N3 = g.N3;
+  const int j0 = blockIdx.x * S;
+  const int y = blockIdx.y;
+  const int run = blockIdx.z;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const float* Ub = a.Ubar + (size_t)run * N3;
+  const float* zc = a.zc;
+  float2* wk = work + (size_t)warp * N1;
+  const int NS = S + 2;
+
+  auto nrow = [&](int f, int s) -> float* { return nod + ((size_t)f * NS + s) * N1; };
+  auto brow = [&](int f, int s) -> float* { return bnod + ((size_t)f * NS + s) * N1; };
+
+  // ---- phase A: inverse transforms of u1,u3 and b,u2 in pairs (ToNodal) ----
+  const int npairs = g.dim3 ? 2 : 2;
+  for (int task = warp; task < NS * npairs; task += kXWarps) {
+    const int s = task / npairs, pr = task - s * npairs;
+    const int t = j0 - 1 + s;
+    const int fA = pr == 0 ? 0 : 3;       // u1 | b
+    const int fB = pr == 0 ? 2 : 1;       // u3 | u2
+    float* rA = nrow(pr == 0 ? 0 : 3, s);
+    float* rB = nrow(pr == 0 ? 2 : 1, s);
+    if (t < 0 || t >= N3) {
+      for (int x = lane; x < N1; x += 32) { rA[x] = 0.f; rB[x] = 0.f; }
+      continue;
+    }
+    const bool hasB = (fB != 1) || g.dim3;
+    const float2* srcA;
+    const float2* srcB;
+    if (g.dim3) {
+      srcA = a.mixin + (((size_t)(run * 4 + fA) * N3 + t) * g.N2 + y) * K1;
+      srcB = a.mixin + (((size_t)(run * 4 + fB) * N3 + t) * g.N2 + y) * K1;
+    } else {
+      srcA = a.S + ((size_t)(run * 5 + fA) * N3 + t) * g.Pp;
+      srcB = a.S + ((size_t)(run * 5 + fB) * N3 + t) * g.Pp;
+    }
+    for (int x = lane; x < N1; x += 32) wk[x] = make_float2(0.f, 0.f);
+    __syncwarp();
+    for (int k = lane; k < K1; k += 32) {
+      float2 A = srcA[k];
+      float2 B = hasB ? srcB[k] : make_float2(0.f, 0.f);
+      if (k == 0) {
+        wk[0] = make_float2(A.x, B.x);  // c2r uses the real part of the k = 0 term
+      } else {
+        wk[k] = make_float2(A.x - B.y, A.y + B.x);        // A + iB
+        wk[N1 - k] = make_float2(A.x + B.y, B.x - A.y);   // conj(A) + i conj(B)
+      }
+    }
+    __syncwarp();
+    warp_fft(wk, N1, g.logN1, a.tw, true, lane);
+    for (int x = lane; x < N1; x += 32) {
+      float2 v = wk[x];
+      rA[x] = v.x;
+      rB[x] = v.y;
+    }
+    __syncwarp();
+  }
+  if (LINEAR) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
+    for (int i = threadIdx.x; i < 4 * NS * N1; i += kXThreads) {
+      int f = i / (NS * N1), r = i - f * NS * N1, s = r / N1, x = r - s * N1;
+      int t = j0 - 1 + s;
+      float v = 0.f;
+      if (t >= 0 && t < N3 && (f != 1 || g.dim3)) {
+        v = a.base[(((size_t)(run * 4 + f) * N3 + t) * g.N2 + y) * N1 + x];
+        if (f == 0) v += Ub[t];
+      }
+      bnod[i] = v;
+    }
+  }
+  __syncthreads();
+
+  // ---- phase B/C: nodal products, forward transforms in pairs (ToModal) ----
+  const int nprod = L.nprod;
+  int nrows = 0;
+  for (int p = 0; p < nprod; p++) { int f0, c; prod_slots(p, S, f0, c); nrows += c; }
+  const int ntask = (nrows + 1) / 2;
+  for (int task = warp; task < ntask; task += kXWarps) {
+    int pp[2], ss[2];
+    bool live[2];
+    for (int h = 0; h < 2; h++) {
+      int r = 2 * task + h;
+      pp[h] = -1; ss[h] = 0; live[h] = false;
+      if (r < nrows) {
+        for (int p = 0; p < nprod; p++) {
+          int f0, c; prod_slots(p, S, f0, c);
+          if (r < c) { pp[h] = p; ss[h] = f0 + r; break; }
+          r -= c;
+        }
+        int t = j0 - 1 + ss[h];
+        live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
+      }
+    }
+    for (int x = lane; x < N1; x += 32) {
+      float v[2];
+      for (int h = 0; h < 2; h++) {
+        v[h] = 0.f;
+        if (!live[h]) continue;
+        const int s = ss[h], t = j0 - 1 + s;
+        const float u1 = nrow(0, s)[x], u2 = nrow(1, s)[x], u3 = nrow(2, s)[x], bb = nrow(3, s)[x];
+        const float ub = Ub[t];
+        const bool lo = (t >= 1) && (s >= 1);   // rows with a level below (Bar, Tilde rows j >= 1)
+        const float u1m = lo ? nrow(0, s - 1)[x] : 0.f;
+        const float u2m = lo ? nrow(1, s - 1)[x] : 0.f;
+        const float bm = lo ? nrow(3, s - 1)[x] : 0.f;
+        const float ubm = lo ? Ub[t - 1] : 0.f;
+        const float tlo = zc[ZC_TILDE_LO * N3 + t], tdi = zc[ZC_TILDE_DI * N3 + t];
+        if (!LINEAR) {
+          const float U1t = u1 + ub, U1tm = u1m + ubm;
+          switch (pp[h]) {
+            // U1t*U1t enters only through ddx (IMEXRK.cpp:155-156); the x-independent
+            // U_^2 part lies in the kx = 0 mode, which ddx multiplies by zero, so
+            // it is left out of the product to keep the FP32 rounding small.
+            case P_S1: v[h] = u1 * (2.f * ub + u1); break;
+            case P_SB1: v[h] = U1t * bb; break;
+            case P_P3: v[h] = lo ? (tlo * U1tm + tdi * U1t) * u3 : 0.f; break;
+            case P_Q1: v[h] = lo ? (0.5f * U1tm + 0.5f * U1t) * u3 : 0.f; break;
+            case P_QB: v[h] = lo ? (0.5f * bm + 0.5f * bb) * u3 : 0.f; break;
+            case P_P4: {
+              float d = (t <= N3 - 2) ? 0.5f * u3 + 0.5f * nrow(2, s + 1)[x] : 0.5f * u3;
+              v[h] = d * d;
+            } break;
+            case P_S12: v[h] = U1t * u2; break;
+            case P_S22: v[h] = u2 * u2; break;
+            case P_SB2: v[h] = u2 * bb; break;
+            case P_Q2: v[h] = lo ? (0.5f * u2m + 0.5f * u2) * u3 : 0.f; break;
+            case P_P3Y: v[h] = lo ? (tlo * u2m + tdi * u2) * u3 : 0.f; break;
+          }
+        } else {
+          const float nn = brow(0, s)[x], u2b = brow(1, s)[x], u3b = brow(2, s)[x], bbb = brow(3, s)[x];
+          const float nnm = lo ? brow(0, s - 1)[x] : 0.f;
+          const float u2bm = lo ? brow(1, s - 1)[x] : 0.f;
+          const float bbm = lo ? brow(3, s - 1)[x] : 0.f;
+          switch (pp[h]) {
+            case P_S1: v[h] = 2.f * (u1 * nn); break;
+            case P_SB1: v[h] = bb * nn + bbb * u1; break;
+            case P_P3: v[h] = lo ? (tlo * u1m + tdi * u1) * u3b + (tlo * nnm + tdi * nn) * u3 : 0.f; break;
+            case P_Q1: v[h] = lo ? (0.5f * u1m + 0.5f * u1) * u3b + (0.5f * nnm + 0.5f * nn) * u3 : 0.f; break;
+            case P_QB: v[h] = lo ? (0.5f * bm + 0.5f * bb) * u3b + (0.5f * bbm + 0.5f * bbb) * u3 : 0.f; break;
+            case P_P4: {
+              float d, db;
+              if (t <= N3 - 2) {
+                d = 0.5f * u3 + 0.5f * nrow(2, s + 1)[x];
+                db = 0.5f * u3b + 0.5f * brow(2, s + 1)[x];
+              } else {
+                d = 0.5f * u3;
+                db = 0.5f * u3b;
+              }
+              v[h] = 2.f * (d * db);
+            } break;
+            case P_S12: v[h] = u1 * u2b + nn * u2; break;
+            case P_S22: v[h] = 2.f * (u2 * u2b); break;
+            case P_SB2: v[h] = bb * u2b + bbb * u2; break;
+            case P_Q2: v[h] = lo ? (0.5f * u2m + 0.5f * u2) * u3b + (0.5f * u2bm + 0.5f * u2b) * u3 : 0.f; break;
+            case P_P3Y: v[h] = lo ? (tlo * u2m + tdi * u2) * u3b + (tlo * u2bm + tdi * u2b) * u3 : 0.f; break;
+          }
+        }
+      }
+      wk[x] = make_float2(v[0], v[1]);
+    }
+    __syncwarp();
+    warp_fft(wk, N1, g.logN1, a.tw, false, lane);
+    const float sc = 0.5f * g.inv_n12;
+    for (int k = lane; k < K1; k += 32) {
+      float2 zk = wk[k];
+      float2 zc2 = cconj(wk[(N1 - k) & (N1 - 1)]);
+      if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
+        hat[((size_t)pp[0] * NS + ss[0]) * K1 + k] = live[0] ? make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc)
+                                                             : make_float2(0.f, 0.f);
+      if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
+        hat[((size_t)pp[1] * NS + ss[1]) * K1 + k] = live[1] ? make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc)
+                                                             : make_float2(0.f, 0.f);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // ---- phase D: z stencils of the products and x derivatives ----
+  auto H = [&](int p, int s, int k) -> float2 { return hat[((size_t)p * NS + s) * K1 + k]; };
+  for (int i = threadIdx.x; i < S * K1; i += kXThreads) {
+    const int si = i / K1, k = i - si * K1;
+    const int t = j0 + si, s = si + 1;
+    if (t >= N3) continue;
+    const float kxv = a.kx[k];
+    // ddz Dirichlet -> Neumann of a Q product (Differentiation.cpp:35-61)
+    auto dzdn = [&](int p) -> float2 {
+      if (t == 0) return make_float2(0.f, 0.f);
+      float di = zc[ZC_DDN_DI * N3 + t];
+      float2 v = cscale(H(p, s, k), di);
+      if (t < N3 - 1) v = cadd(v, cscale(H(p, s + 1, k), zc[ZC_DDN_UP * N3 + t]));
+      return v;
+    };
+    float2 dnd = make_float2(0.f, 0.f);  // ddz Neumann -> Dirichlet of P4
+    if (t >= 2)
+      dnd = cadd(cscale(H(P_P4, s - 1, k), zc[ZC_DND_LO * N3 + t]), cscale(H(P_P4, s, k), zc[ZC_DND_DI * N3 + t]));
+    const float2 c1 = csub(cscale(cik(kxv, H(P_S1, s, k)), -1.f), dzdn(P_Q1));
+    const float2 c3 = csub(cscale(cik(kxv, H(P_P3, s, k)), -1.f), dnd);
+    const float2 cB = csub(cscale(cik(kxv, H(P_SB1, s, k)), -1.f), dzdn(P_QB));
+    if (!g.dim3) {
+      float2* r = a.rnl + (size_t)run * 4 * g.fblk + (size_t)t * g.Pp + k;
+      r[0 * g.fblk] = c1;
+      r[2 * g.fblk] = c3;
+      r[3 * g.fblk] = cB;
+    } else {
+      const float2 c1y = cscale(H(P_S12, s, k), -1.f);
+      const float2 c2 = csub(cscale(cik(kxv, H(P_S12, s, k)), -1.f), dzdn(P_Q2));
+      const float2 c2y = cscale(H(P_S22, s, k), -1.f);
+      const float2 c3y = cscale(H(P_P3Y, s, k), -1.f);
+      const float2 cBy = cscale(H(P_SB2, s, k), -1.f);
+      float2* m = a.mixout + (((size_t)run * 8 * N3 + t) * g.N2 + y) * K1 + k;
+      const size_t cs = g.mblk;
+      m[0 * cs] = c1; m[1 * cs] = c1y; m[2 * cs] = c2; m[3 * cs] = c2y;
+      m[4 * cs] = c3; m[5 * cs] = c3y; m[6 * cs] = cB; m[7 * cs] = cBy;
+    }
+  }
+}
+
+// ============================================================ z pass ====
+constexpr int kZThreads = 128;
+constexpr int kZU = 8;   // levels of every input loaded ahead per thread
+
+
+// ExplicitRK (IMEXRK.cpp:119-134), the linear terms of BuildRHS (:140-147),
+// FinishRHS (:107-117), CrankNicolson (:75-98) and the Thomas solve
+// (Tridiagonal.h:29-53) for one (run, mode, field, real|imag component):
+// the factors are real, so the real and imaginary parts are independent
+// solves (Field.h:519-531). The forward sweep loads kZU levels of every input
+// into registers before using them, stores D_j in the next state, and the
+// backward sweep overwrites D_j with the solution.
+__global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
+  const Geo g = a.g;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int m = t >> 1, c = t & 1;
+  const int run = blockIdx.z;
+  if (m >= g.P) return;
+  const int fi = blockIdx.y;
+  const int f = g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
+  const int N3 = g.N3, Pp = g.Pp;
+  const int q = m / g.K1, j1 = m - q * g.K1;
+  const float kxv = a.kx[j1], kyv = a.ky[q];
+  const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
+  const float sc = c == 0 ? -1.f : 1.f;   // (i k z)_c = sc * k * z_{1-c}
+  const bool dir = (f == 2);
+  const int fam = (f == 3) ? 1 : (dir ? 2 : 0);
+  const int fs = fam * 3 + a.stage;
+  const float* __restrict__ fa = a.fa + (size_t)fs * N3;
+  const float* __restrict__ fc = a.fc + (size_t)fs * N3;
+  const float* __restrict__ iden = a.inv_den + (size_t)fs * N3 * Pp + m;
+  const float* __restrict__ zc = a.zc;
+  const float* __restrict__ lo2 = zc + (dir ? ZC_D2D_LO : ZC_D2N_LO) * N3;
+  const float* __restrict__ di2 = zc + (dir ? ZC_D2D_DI : ZC_D2N_DI) * N3;
+  const float* __restrict__ up2 = zc + (dir ? ZC_D2D_UP : ZC_D2N_UP) * N3;
+  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
+  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
+  const float* __restrict__ full_lo = zc + ZC_FULL_LO * N3;
+  const float* __restrict__ full_di = zc + ZC_FULL_DI * N3;
+  const float cco = (f == 3) ? a.cb : a.cv;
+  const float Ri = a.Ri[run];
+  const float* __restrict__ dB = a.dBdz + (size_t)run * N3;
+  const bool zmode = (m == 0);   // the (0,0) mode: no buoyancy force (IMEXRK.cpp:141-143)
+
+  const float2* __restrict__ u = a.S + ((size_t)(run * 5 + f) * N3) * Pp + m;
+  const float2* __restrict__ pp = a.S + ((size_t)(run * 5 + 4) * N3) * Pp + m;
+  const float2* __restrict__ bsrc = a.S + ((size_t)(run * 5 + 3) * N3) * Pp + m;
+  const float2* __restrict__ u3s = a.S + ((size_t)(run * 5 + 2) * N3) * Pp + m;
+  const float2* __restrict__ rnl = a.rnl + ((size_t)(run * 4 + f) * N3) * Pp + m;
+  float* __restrict__ rold = reinterpret_cast<float*>(a.rold + ((size_t)(run * 4 + f) * N3) * Pp + m) + c;
+  float* __restrict__ out = reinterpret_cast<float*>(a.Sn + ((size_t)(run * 5 + f) * N3) * Pp + m) + c;
+  const float* uc = reinterpret_cast<const float*>(u) + c;
+  const float* pc = reinterpret_cast<const float*>(pp) + c;           // p_c
+  const float* po = reinterpret_cast<const float*>(pp) + (1 - c);     // p_{1-c}
+  const float* bc = reinterpret_cast<const float*>(bsrc) + c;
+  const float* wc = reinterpret_cast<const float*>(u3s) + c;
+  const float* rc = reinterpret_cast<const float*>(rnl) + c;
+  const bool use_rold = (a.hz != 0.f);
+  const float kgrad = (f == 0) ? kxv : kyv;
+
+  float um = 0.f, u0 = uc[0];
+  float pm1 = 0.f, bm1 = 0.f, w0 = wc[0];
+  float Dprev = 0.f;
+  for (int j0 = 0; j0 < N3; j0 += kZU) {
+    float bu[kZU], br[kZU], bo[kZU], bp[kZU], bx[kZU], bi[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      const bool in = j < N3, nx = j + 1 < N3;
+      bu[i] = nx ? uc[2 * (size_t)(j + 1) * Pp] : 0.f;
+      br[i] = in ? rc[2 * (size_t)j * Pp] : 0.f;
+      bo[i] = (in && use_rold) ? rold[2 * (size_t)j * Pp] : 0.f;
+      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
+      bp[i] = 0.f;
+      bx[i] = 0.f;
+      if (f <= 1) bp[i] = in ? po[2 * (size_t)j * Pp] : 0.f;
+      if (f == 2) {
+        bp[i] = in ? pc[2 * (size_t)j * Pp] : 0.f;
+        bx[i] = in ? bc[2 * (size_t)j * Pp] : 0.f;
+      }
+      if (f == 3) bx[i] = nx ? wc[2 * (size_t)(j + 1) * Pp] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      if (j >= N3) break;
+      const float up = bu[i];
+      float rt = br[i];
+      float gp = 0.f;
+      if (f <= 1) {
+        gp = sc * kgrad * bp[i];   // (i k p)_c
+      } else if (f == 2) {
+        if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
+        pm1 = bp[i];
+        if (j >= 1 && !zmode) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
+        bm1 = bx[i];
+      } else {
+        const float w1 = bx[i];
+        const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
+        rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
+        w0 = w1;
+      }
+      float R = u0;
+      if (use_rold) R += a.hz * bo[i];
+      R += -a.h * gp;
+      R += a.hb * rt;
+      const bool band = dir ? (j >= 2 && j <= N3 - 2) : (j >= 1 && j <= N3 - 2);
+      const float d2u = band ? lo2[j] * um + di2[j] * u0 + up2[j] * up : 0.f;
+      R += cco * ((d1 * u0 + d2 * u0) + d2u);
+      const bool zend = (j <= 1) || (j >= N3 - 2) || (dir && j == 2);   // ZeroEnds (Field.h:475-486)
+      if (zend) R = 0.f;
+      const float D = (j == 0) ? R * bi[i] : (R - fa[j] * Dprev) * bi[i];
+      out[2 * (size_t)j * Pp] = D;
+      rold[2 * (size_t)j * Pp] = rt;
+      Dprev = D;
+      um = u0;
+      u0 = up;
+    }
+  }
+  float x = Dprev;
+  for (int jt = N3 - 2; jt >= 0; jt -= kZU) {
+    float bd[kZU], bi[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = jt - i;
+      bd[i] = j >= 0 ? out[2 * (size_t)j * Pp] : 0.f;
+      bi[i] = j >= 0 ? iden[(size_t)j * Pp] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = jt - i;
+      if (j < 0) break;
+      x = bd[i] - (fc[j] * bi[i]) * x;
+      out[2 * (size_t)j * Pp] = x;
+    }
+  }
+}
+
+// RemoveDivergence (IMEXRK.cpp:43-73) for one (run, mode, component):
+// div = ddx u1 + ddy u2 + ddz u3, ZeroEnds, Laplacian Thomas solve,
+// u -= grad q, p += pm q. The two components of a mode sit in adjacent lanes,
+// which exchange q for the x/y gradients. u1,u2,u3 are updated in place in
+// `U`; p is read from `Psrc` and written to `Pdst`. No thread exits before
+// the shuffles: lanes past the last mode work on a clamped copy and store
+// nothing.
+__global__ void __launch_bounds__(kZThreads) k_z_proj(Geo g, float2* U, const float2* Psrc, float2* Pdst,
+                                                   float2* qbuf, const float* zc, const float* fa,
+                                                   const float* fc, const float* inv_den,
+                                                   const float* kx, const float* ky, float pm) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int run = blockIdx.z;
+  const bool act = (t >> 1) < g.P;
+  const int m = act ? (t >> 1) : 0, c = t & 1;
+  const int N3 = g.N3, Pp = g.Pp;
+  const int q = m / g.K1, j1 = m - q * g.K1;
+  const float kxv = kx[j1], kyv = g.dim3 ? ky[q] : 0.f;
+  const float sc = c == 0 ? -1.f : 1.f;
+  float* u1 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 0) * N3) * Pp + m);
+  float* u2 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 1) * N3) * Pp + m);
+  float* u3 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 2) * N3) * Pp + m) + c;
+  const float* ps = reinterpret_cast<const float*>(Psrc + ((size_t)(run * 5 + 4) * N3) * Pp + m) + c;
+  float* pd = reinterpret_cast<float*>(Pdst + ((size_t)(run * 5 + 4) * N3) * Pp + m) + c;
+  float* qb = reinterpret_cast<float*>(qbuf + (size_t)run * N3 * Pp + m) + c;
+  const float* __restrict__ a_ = fa + (size_t)kFS_Lap * N3;
+  const float* __restrict__ c_ = fc + (size_t)kFS_Lap * N3;
+  const float* __restrict__ iden = inv_den + (size_t)kFS_Lap * N3 * Pp + m;
+  const float* __restrict__ ddn_di = zc + ZC_DDN_DI * N3;
+  const float* __restrict__ ddn_up = zc + ZC_DDN_UP * N3;
+  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
+  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
+  const float* u1o = u1 + (1 - c);   // u1_{1-c}
+  const float* u2o = u2 + (1 - c);
+  float* u1c = u1 + c;
+  float* u2c = u2 + c;
+
+  float w0 = u3[0];
+  float Dprev = 0.f;
+  for (int j0 = 0; j0 < N3; j0 += kZU) {
+    float b1[kZU], b2[kZU], b3[kZU], bi[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      const bool in = j < N3;
+      b1[i] = in ? u1o[2 * (size_t)j * Pp] : 0.f;
+      b2[i] = (in && g.dim3) ? u2o[2 * (size_t)j * Pp] : 0.f;
+      b3[i] = (j + 1 < N3) ? u3[2 * (size_t)(j + 1) * Pp] : 0.f;
+      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      if (j >= N3) break;
+      const float w1 = b3[i];
+      float dv = 0.f;
+      if (j >= 2 && j <= N3 - 3) dv = sc * (kxv * b1[i] + kyv * b2[i]) + (ddn_di[j] * w0 + ddn_up[j] * w1);
+      const float D = (j == 0) ? dv * bi[i] : (dv - a_[j] * Dprev) * bi[i];
+      if (act) qb[2 * (size_t)j * Pp] = D;
+      Dprev = D;
+      w0 = w1;
+    }
+  }
+  // backward sweep: q_j, then u1_j, u2_j, p_j and u3_{j+1}
+  float qn = Dprev;   // q_{N-1}
+  {
+    const int j = N3 - 1;
+    const float qo = __shfl_xor_sync(0xffffffffu, qn, 1);
+    if (act) {
+      u1c[2 * (size_t)j * Pp] -= sc * kxv * qo;
+      if (g.dim3) u2c[2 * (size_t)j * Pp] -= sc * kyv * qo;
+      pd[2 * (size_t)j * Pp] = ps[2 * (size_t)j * Pp] + pm * qn;
+    }
+  }
+  for (int jt = N3 - 2; jt >= 0; jt -= kZU) {
+    float bq[kZU], bi[kZU], b1[kZU], b2[kZU], b3[kZU], bp[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = jt - i;
+      const bool in = j >= 0;
+      bq[i] = in ? qb[2 * (size_t)j * Pp] : 0.f;
+      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
+      b1[i] = in ? u1c[2 * (size_t)j * Pp] : 0.f;
+      b2[i] = (in && g.dim3) ? u2c[2 * (size_t)j * Pp] : 0.f;
+      b3[i] = in ? u3[2 * (size_t)(j + 1) * Pp] : 0.f;
+      bp[i] = in ? ps[2 * (size_t)j * Pp] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = jt - i;
+      if (j < 0) break;
+      float Cj = c_[j] * bi[i];
+      if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
+      const float qj = bq[i] - Cj * qn;
+      const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
+      if (act) {
+        u1c[2 * (size_t)j * Pp] = b1[i] - sc * kxv * qo;
+        if (g.dim3) u2c[2 * (size_t)j * Pp] = b2[i] - sc * kyv * qo;
+        pd[2 * (size_t)j * Pp] = bp[i] + pm * qj;
+        const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
+        if (jj >= 2) u3[2 * (size_t)jj * Pp] = b3[i] - (dnd_lo[jj] * qj + dnd_di[jj] * qn);
+      }
+      qn = qj;
+    }
+  }
+}
+
+// ====================================================== factorisation ====
+// Thomas factors of every (factor set, mode) in FP64 (Tridiagonal.h:14-27):
+// inv_den_j = 1/(b_j - a_j C_{j-1}), stored as float. Rows follow
+// UpdateForTimestep (IMEXRK.h:502-545) and the Laplacian of the constructor
+// (IMEXRK.h:55-78) with Neumannify / Dirichlify (Differentiation.h:17-59).
+__global__ void k_factor(Geo g, const double* __restrict__ bands, const double* __restrict__ kx,
+                         const double* __restrict__ ky, double h0, double h1, double h2, double Re,
+                         double Pr, float* inv_den) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fs = blockIdx.y;
+  const int N = g.N3;
+  if (m >= g.Pp) return;
+  float* out = inv_den + (size_t)fs * N * g.Pp + m;
+  if (m >= g.P) {
+    for (int j = 0; j < N; j++) out[(size_t)j * g.Pp] = 0.f;
+    return;
+  }
+  const int q = m / g.K1, j1 = m - q * g.K1;
+  const double kk = -(kx[j1] * kx[j1]) + -(ky[q] * ky[q]);
+  const bool lap = (fs == kFS_Lap);
+  const int fam = lap ? 0 : fs / 3, k = lap ? 0 : fs % 3;
+  const bool dir = (fam == 2);
+  const double h = k == 0 ? h0 : (k == 1 ? h1 : h2);
+  const double s = 0.5 * h;
+  const double den_re = (fam == 1) ? Re * Pr : Re;
+  const double* lo = bands + (dir ? 3 : 0) * N;
+  const double* di = bands + (dir ? 4 : 1) * N;
+  const double* up = bands + (dir ? 5 : 2) * N;
+  double Cprev = 0.0;
+  for (int j = 0; j < N; j++) {
+    double aj, bj, cj;
+    if (lap) {
+      aj = lo[j]; bj = di[j] + kk; cj = up[j];
+    } else {
+      aj = -(s * lo[j]) / den_re; bj = 1.0 - (s * (di[j] + kk)) / den_re; cj = -(s * up[j]) / den_re;
+    }
+    if (!dir) {   // Neumannify
+      if (j == 0) { bj = 1; cj = 0; }
+      if (j == 1) { aj = 0; bj = 1; cj = -1; }
+      if (j == N - 2) { aj = 1; bj = -1; cj = 0; }
+      if (j == N - 1) { aj = 0; bj = 1; cj = 0; }
+      if (lap && m == 0 && j == 1) cj = 0;   // (0,0) mode pinned
+    } else {      // Dirichlify
+      if (j <= 2) { aj = 0; bj = 1; cj = 0; }
+      if (j >= N - 2) { aj = 0; bj = 1; cj = 0; }
+    }
+    if (j == N - 1) cj = 0;
+    double den = (j == 0) ? bj : bj - aj * Cprev;
+    out[(size_t)j * g.Pp] = (float)(1.0 / den);
+    Cprev = cj / den;
+  }
+}
+
+// ============================================== layout transposes ====
+// reference layout [N2][M1][N3] (z fastest) <-> kept layout [N3][Pp]
+__global__ void k_gather_ref(Geo g, const float2* __restrict__ ref, float2* __restrict__ kept) {
+  __shared__ float2 tile[32][33];
+  const int M1 = g.N1 / 2 + 1;
+  const int m0 = blockIdx.x * 32, jz0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int m = m0 + r, jz = jz0 + threadIdx.x;
+    float2 v = make_float2(0.f, 0.f);
+    if (m < g.P && jz < g.N3) {
+      int q = m / g.K1, j1 = m - q * g.K1;
+      int n2 = n2_of_q(q, g.Ky, g.K2, g.N2);
+      v = ref[((size_t)M1 * n2 + j1) * g.N3 + jz];
+    }
+    tile[r][threadIdx.x] = v;
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int jz = jz0 + r, m = m0 + threadIdx.x;
+    if (jz < g.N3 && m < g.Pp) kept[(size_t)jz * g.Pp + m] = tile[threadIdx.x][r];
+  }
+}
+
+__global__ void k_scatter_ref(Geo g, const float2* __restrict__ kept, float2* __restrict__ ref) {
+  __shared__ float2 tile[32][33];
+  const int M1 = g.N1 / 2 + 1;
+  const int m0 = blockIdx.x * 32, jz0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int jz = jz0 + r, m = m0 + threadIdx.x;
+    tile[threadIdx.x][r] = (jz < g.N3 && m < g.P) ? kept[(size_t)jz * g.Pp + m] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+    int m = m0 + r, jz = jz0 + threadIdx.x;
+    if (m < g.P && jz < g.N3) {
+      int q = m / g.K1, j1 = m - q * g.K1;
+      int n2 = n2_of_q(q, g.Ky, g.K2, g.N2);
+      ref[((size_t)M1 * n2 + j1) * g.N3 + jz] = tile[r][threadIdx.x];
+    }
+  }
+}
+
+// ============================================================ energies ====
+// InnerProd (Integration.h:282-311) of each field pair in FP64: per level the
+// sum over kept modes of w_m Re(a conj b) with w = 1 for (0,0) and 2 otherwise,
+// then the vertical quadrature. out[pair*4 + f] accumulates field f
+// (0 u1, 1 u2, 2 u3, 3 b).
+__global__ void k_inner(Geo g, const float2* __restrict__ Sa, const float2* __restrict__ Sb,
+                        const float* __restrict__ zc, double* out) {
+  const int j = blockIdx.x;
+  const int pair = blockIdx.y;
+  const int f = blockIdx.z;
+  const float2* a = Sa + ((size_t)(pair * 5 + f) * g.N3 + j) * g.Pp;
+  const float2* b = Sb + ((size_t)(pair * 5 + f) * g.N3 + j) * g.Pp;
+  double s = 0.0;
+  for (int m = threadIdx.x; m < g.P; m += blockDim.x) {
+    float2 x = a[m], y = b[m];
+    double v = (double)x.x * y.x + (double)x.y * y.y;
+    s += (m == 0) ? v : 2.0 * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    const float wz = zc[(f == 2 ? ZC_WZD : ZC_WZN) * g.N3 + j];
+    if (wz != 0.f) atomicAdd(out + pair * 4 + f, t * (double)wz);
+  }
+}
+
+// ======================================================== launchers ====
+static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+static int launch_xpass(const StageArgs& a, cudaStream_t st) {
+  const Geo& g = a.g;
+  // slab of output levels per block: the largest of 8, 4, 2 whose shared
+  // memory fits in one SM's opt-in limit
+  int S = 8;
+  for (; S > 2; S >>= 1)
+    if (x_layout(S, g.N1, g.K1, g.dim3, a.linear).bytes <= 200 * 1024) break;
+  if (g.dim3 && S > 4) S = 4;
+  size_t sm = x_layout(S, g.N1, g.K1, g.dim3, a.linear).bytes;
+  dim3 grid(cdiv(g.N3, S), g.N2, g.nrun);
+#define XCASE(SV, LIN) k_xpass<SV, LIN><<<grid, kXThreads, sm, st>>>(a);
+  if (a.linear) {
+    if (S == 8) XCASE(8, true) else if (S == 4) XCASE(4, true) else XCASE(2, true)
+  } else {
+    if (S == 8) XCASE(8, false) else if (S == 4) XCASE(4, false) else XCASE(2, false)
+  }
+#undef XCASE
+  return 1;
+}
+
+// opt-in shared-memory limits of every kernel, set once per process before
+// any launch (and outside stream capture)
+int prepare_kernels() {
+  const int lim = 227 * 1024;
+  cudaError_t e = cudaSuccess;
+#define ATTR(K) if (e == cudaSuccess) e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  ATTR(k_ifft_y) ATTR(k_fft_y)
+  ATTR((k_xpass<8, false>)) ATTR((k_xpass<4, false>)) ATTR((k_xpass<2, false>))
+  ATTR((k_xpass<8, true>)) ATTR((k_xpass<4, true>)) ATTR((k_xpass<2, true>))
+#undef ATTR
+  return e == cudaSuccess ? 0 : -1;
+}
+
+int launch_project(const StageArgs& a, cudaStream_t st) {
+  const Geo& g = a.g;
+  dim3 grid(cdiv(2 * g.P, kZThreads), 1, g.nrun);
+  k_z_proj<<<grid, kZThreads, 0, st>>>(g, a.Sn, a.S, a.Sn, a.qbuf, a.zc, a.fa, a.fc, a.inv_den, a.kx, a.ky,
+                                       a.pm);
+  return 1;
+}
+
+const char* stage_kernel_name(const Geo& g, int i) {
+  static const char* n3[] = {"k_ifft_y", "k_xpass", "k_fft_y", "k_z_cn", "k_z_proj"};
+  static const char* n2[] = {"k_xpass", "k_z_cn", "k_z_proj"};
+  return g.dim3 ? n3[i] : n2[i];
+}
+int stage_kernel_count(const Geo& g) { return g.dim3 ? 5 : 3; }
+
+int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+  const Geo& g = a.g;
+  int n = 0;
+  auto mark = [&]() {
+    if (ev) cudaEventRecord(ev[n], st);
+    n++;
+  };
+  if (g.dim3) {
+    size_t sm = sizeof(float2) * kCG * (g.N2 + 1);
+    k_ifft_y<<<dim3(cdiv(g.K1, kCG), g.N3, g.nrun * 4), kYThreads, sm, st>>>(a);
+    mark();
+  }
+  launch_xpass(a, st);
+  mark();
+  if (g.dim3) {
+    size_t sm = sizeof(float2) * 2 * kCG * (g.N2 + 1);
+    k_fft_y<<<dim3(cdiv(g.K1, kCG), g.N3, g.nrun * 4), kYThreads, sm, st>>>(a);
+    mark();
+  }
+  k_z_cn<<<dim3(cdiv(2 * g.P, kZThreads), g.dim3 ? 4 : 3, g.nrun), kZThreads, 0, st>>>(a);
+  mark();
+  launch_project(a, st);
+  mark();
+  return n;
+}
+
+int launch_factor(const Geo& g, const double* bands, const double* kx, const double* ky, double h0, double h1,
+                  double h2, double Re, double Pr, float* inv_den, cudaStream_t st) {
+  k_factor<<<dim3(cdiv(g.Pp, 128), kNumFS), 128, 0, st>>>(g, bands, kx, ky, h0, h1, h2, Re, Pr, inv_den);
+  return 1;
+}
+
+int launch_gather_ref(const Geo& g, const float2* ref, float2* kept, cudaStream_t st) {
+  k_gather_ref<<<dim3(cdiv(g.Pp, 32), cdiv(g.N3, 32)), dim3(32, 8), 0, st>>>(g, ref, kept);
+  return 1;
+}
+
+int launch_scatter_ref(const Geo& g, const float2* kept, float2* ref, cudaStream_t st) {
+  k_scatter_ref<<<dim3(cdiv(g.P, 32), cdiv(g.N3, 32)), dim3(32, 8), 0, st>>>(g, kept, ref);
+  return 1;
+}
+
+int launch_energy(const Geo& g, const float2* Sa, const float2* Sb, int npairs, const float* zc, const float* Ri,
+                  double* out, cudaStream_t st) {
+  (void)Ri;
+  k_inner<<<dim3(g.N3, npairs, 4), 256, 0, st>>>(g, Sa, Sb, zc, out);
+  return 1;
+}
+
+// nodal field of one modal field (kept layout, one run) -> base [N3][N2][N1]
+// via the same transforms as the x pass: used once per set_base.
+__global__ void k_base_x(Geo g, const float2* __restrict__ rows, long long row_stride_level,
+                         long long row_stride_y, float* __restrict__ out, const float2* __restrict__ tw) {
+  extern __shared__ float2 wsm[];
+  const int t = blockIdx.x, y = blockIdx.y;
+  const int lane = threadIdx.x;
+  float2* wk = wsm;
+  const float2* src = rows + (size_t)t * row_stride_level + (size_t)y * row_stride_y;
+  for (int x = lane; x < g.N1; x += 32) wk[x] = make_float2(0.f, 0.f);
+  __syncwarp();
+  for (int k = lane; k < g.K1; k += 32) {
+    float2 A = src[k];
+    if (k == 0) wk[0] = make_float2(A.x, 0.f);
+    else { wk[k] = A; wk[g.N1 - k] = cconj(A); }
+  }
+  __syncwarp();
+  warp_fft(wk, g.N1, g.logN1, tw, true, lane);
+  float* o = out + ((size_t)t * g.N2 + y) * g.N1;
+  for (int x = lane; x < g.N1; x += 32) o[x] = wk[x].x;
+}
+
+int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* base_out, const float2* tw,
+                      float* scratch_mixed, cudaStream_t st) {
+  (void)field;
+  if (!g.dim3) {
+    k_base_x<<<dim3(g.N3, 1), 32, sizeof(float2) * g.N1, st>>>(g, kept_modal, g.Pp, 0, base_out, tw);
+    return 1;
+  }
+  // 3D: inverse y transform into scratch [N3][N2][K1], then x
+  StageArgs a = {};
+  a.g = g;
+  a.g.nrun = 1;
+  a.S = kept_modal;   // treated as field 0 of a one-run state
+  a.mixin = reinterpret_cast<float2*>(scratch_mixed);
+  a.tw = tw;
+  size_t sm = sizeof(float2) * kCG * (g.N2 + 1);
+  k_ifft_y<<<dim3(cdiv(g.K1, kCG), g.N3, 1), kYThreads, sm, st>>>(a);
+  k_base_x<<<dim3(g.N3, g.N2), 32, sizeof(float2) * g.N1, st>>>(g, a.mixin, (long long)g.N2 * g.K1, g.K1,
+                                                                base_out, tw);
+  return 2;
+}
+
+}  // namespace sf

@@ -1,0 +1,627 @@
+// C-ABI of the B200 IMEX-RK engine: solver set-up, state transfer, and the
+// step sequencer (one CUDA graph per step, replayed).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/stratiflow_b200.h"
+#include "sf_internal.cuh"
+
+using namespace sf;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                              \
+  do {                                                                                        \
+    cudaError_t e__ = (call);                                                                 \
+    if (e__ != cudaSuccess)                                                                   \
+      return fail(SF_ECUDA, std::string(#call) + ": " + cudaGetErrorString(e__));             \
+  } while (0)
+
+struct sf_solver {
+  Geo g{};
+  int device = 0;
+  cudaStream_t st = nullptr;
+  double L1 = 0, L2 = 0, L3 = 0, Re = 0, Pr = 0, dt = 0;
+  float h[3] = {0, 0, 0};
+  // device buffers
+  float2* S[2] = {nullptr, nullptr};
+  float2 *rold = nullptr, *rnl = nullptr, *qbuf = nullptr, *mixin = nullptr, *mixout = nullptr;
+  float* base = nullptr;
+  float *zc = nullptr, *fa = nullptr, *fc = nullptr, *inv_den = nullptr;
+  float *kx = nullptr, *ky = nullptr, *Ri = nullptr, *Ubar = nullptr, *dBdz = nullptr;
+  double *bands = nullptr, *kxd = nullptr, *kyd = nullptr, *red = nullptr;
+  float2* tw = nullptr;
+  float2* stage_ref = nullptr;   // one field in the reference layout
+  std::vector<float> hRi;
+  std::vector<double> zN, zfN;   // grid (for inspection)
+  int cur = 0;                   // index of the current state buffer
+  bool base_set = false;
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
+  long long launches = 0;
+  long long launches_per_step[2] = {0, 0};
+};
+
+static const double kBeta[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0};     // IMEXRK.h:631
+static const double kZeta[3] = {0.0, -17.0 / 8.0, -5.0 / 4.0};   // IMEXRK.h:632
+
+static bool pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+static int ilog2(int n) { int l = 0; while ((1 << l) < n) l++; return l; }
+
+// k(n) of Differentiation.cpp:113-132
+static std::vector<double> kint(int n) {
+  std::vector<double> k(n, 0.0);
+  if (n == 1) return k;
+  int idx = 0;
+  for (int v = 0; v <= n / 3; v++) k[idx++] = v;
+  for (int v = 0; v < n - 2 * (n / 3) - 1; v++) k[idx++] = 0;
+  for (int v = -n / 3; v <= -1; v++) k[idx++] = v;
+  return k;
+}
+
+static void free_all(sf_solver* s) {
+  for (int l = 0; l < 2; l++)
+    for (int p = 0; p < 2; p++)
+      if (s->graph[l][p]) cudaGraphExecDestroy(s->graph[l][p]);
+  void* ptrs[] = {s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
+                  s->fc, s->inv_den, s->kx, s->ky, s->Ri, s->Ubar, s->dBdz, s->bands, s->kxd, s->kyd,
+                  s->red, s->tw, s->stage_ref};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (s->st) cudaStreamDestroy(s->st);
+}
+
+static void drop_graphs(sf_solver* s) {
+  for (int l = 0; l < 2; l++)
+    for (int p = 0; p < 2; p++)
+      if (s->graph[l][p]) {
+        cudaGraphExecDestroy(s->graph[l][p]);
+        s->graph[l][p] = nullptr;
+      }
+}
+
+// Tridiagonal rows of every factor set, per row only (a_j, c_j), following
+// UpdateForTimestep (IMEXRK.h:502-545) and the Laplacian (IMEXRK.h:55-78).
+static void build_rows(const sf_solver* s, const std::vector<double>& b6, std::vector<float>& fa,
+                       std::vector<float>& fc) {
+  const int N = s->g.N3;
+  fa.assign((size_t)kNumFS * N, 0.f);
+  fc.assign((size_t)kNumFS * N, 0.f);
+  for (int fs = 0; fs < kNumFS; fs++) {
+    const bool lap = fs == kFS_Lap;
+    const int fam = lap ? 0 : fs / 3, k = lap ? 0 : fs % 3;
+    const bool dir = fam == 2;
+    const double sh = 0.5 * (double)s->h[k];
+    const double dre = fam == 1 ? s->Re * s->Pr : s->Re;
+    const double* lo = &b6[(dir ? 3 : 0) * N];
+    const double* up = &b6[(dir ? 5 : 2) * N];
+    for (int j = 0; j < N; j++) {
+      double a = lap ? lo[j] : -(sh * lo[j]) / dre;
+      double c = lap ? up[j] : -(sh * up[j]) / dre;
+      if (!dir) {
+        if (j == 0) c = 0;
+        if (j == 1) { a = 0; c = -1; }
+        if (j == N - 2) { a = 1; c = 0; }
+        if (j == N - 1) { a = 0; c = 0; }
+      } else {
+        if (j <= 2 || j >= N - 2) { a = 0; c = 0; }
+      }
+      if (j == 0) a = 0;
+      fa[(size_t)fs * N + j] = (float)a;
+      fc[(size_t)fs * N + j] = (float)c;
+    }
+  }
+}
+
+static int refactor(sf_solver* s) {
+  // IMEXRK.h:506-508: h = deltaT * {8,2,5}/15, stored in stratifloat
+  s->h[0] = (float)(s->dt * 8.0 / 15.0);
+  s->h[1] = (float)(s->dt * 2.0 / 15.0);
+  s->h[2] = (float)(s->dt * 5.0 / 15.0);
+  const int N = s->g.N3;
+  std::vector<double> b6(6 * (size_t)N);
+  CK(cudaMemcpy(b6.data(), s->bands, sizeof(double) * 6 * N, cudaMemcpyDeviceToHost));
+  std::vector<float> fa, fc;
+  build_rows(s, b6, fa, fc);
+  CK(cudaMemcpyAsync(s->fa, fa.data(), sizeof(float) * fa.size(), cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->fc, fc.data(), sizeof(float) * fc.size(), cudaMemcpyHostToDevice, s->st));
+  s->launches += launch_factor(s->g, s->bands, s->kxd, s->kyd, s->h[0], s->h[1], s->h[2], s->Re, s->Pr,
+                               s->inv_den, s->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s->st));
+  drop_graphs(s);
+  return SF_OK;
+}
+
+static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
+  StageArgs a{};
+  a.g = s->g;
+  a.S = s->S[cur];
+  a.Sn = s->S[1 - cur];
+  a.rold = s->rold;
+  a.rnl = s->rnl;
+  a.qbuf = s->qbuf;
+  a.mixin = s->mixin;
+  a.mixout = s->mixout;
+  a.zc = s->zc;
+  a.fa = s->fa;
+  a.fc = s->fc;
+  a.inv_den = s->inv_den;
+  a.kx = s->kx;
+  a.ky = s->ky;
+  a.Ri = s->Ri;
+  a.Ubar = s->Ubar;
+  a.dBdz = s->dBdz;
+  a.tw = s->tw;
+  a.base = s->base;
+  a.stage = k;
+  a.linear = linear ? 1 : 0;
+  const float h = s->h[k];
+  a.h = h;
+  a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
+  a.hb = h * (float)kBeta[k];
+  a.cv = 0.5f * h / (float)s->Re;
+  a.cb = 0.5f * h / (float)s->Re / (float)s->Pr;
+  a.pm = 1.0f / h;             // RemoveDivergence(1/h[k])
+  return a;
+}
+
+// one IMEXRK::TimeStep (IMEXRK.cpp:8-24) starting from state buffer `par`
+static int record_step(sf_solver* s, int par, bool linear) {
+  int n = 0;
+  int cur = par;
+  for (int k = 0; k < 3; k++) {
+    StageArgs a = stage_args(s, k, cur, linear);
+    n += launch_stage(a, s->st);
+    cur = 1 - cur;
+  }
+  return n;
+}
+
+static int ensure_graph(sf_solver* s, bool linear, int par) {
+  if (s->graph[linear][par]) return SF_OK;
+  cudaGraph_t gr;
+  CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+  int n = record_step(s, par, linear);
+  cudaError_t e = cudaStreamEndCapture(s->st, &gr);
+  if (e != cudaSuccess) return fail(SF_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&s->graph[linear][par], gr, 0);
+  cudaGraphDestroy(gr);
+  if (e != cudaSuccess) return fail(SF_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  s->launches_per_step[linear] = n;
+  return SF_OK;
+}
+
+extern "C" {
+
+const char* sf_last_error(void) { return g_err.c_str(); }
+
+int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, sf_solver** out) {
+  if (!grid || !flow || !out) return fail(SF_EINVAL, "null argument");
+  const int N1 = grid->N1, N2 = grid->N2, N3 = grid->N3, nrun = grid->nrun;
+  if (!pow2(N1) || N1 < 16 || N1 > kMaxN) return fail(SF_EINVAL, "N1 must be a power of two in [16,512]");
+  if (!(N2 == 1 || (pow2(N2) && N2 >= 16 && N2 <= 256)))
+    return fail(SF_EINVAL, "N2 must be 1 or a power of two in [16,256]");
+  if (N3 % 4 != 0 || N3 < 16 || N3 > 1024) return fail(SF_EINVAL, "N3 must be a multiple of 4 in [16,1024]");
+  if (nrun < 1) return fail(SF_EINVAL, "nrun must be >= 1");
+  if (!(dt > 0) || !(flow->Re > 0) || !(flow->Pr > 0) || !(flow->L1 > 0) || !(flow->L3 > 0) ||
+      (N2 > 1 && !(flow->L2 > 0)))
+    return fail(SF_EINVAL, "dt, Re, Pr, L1, L3 (and L2 in 3D) must be positive");
+  CK(cudaSetDevice(device));
+  sf_solver* s = new sf_solver();
+  s->device = device;
+  s->L1 = flow->L1; s->L2 = flow->L2; s->L3 = flow->L3; s->Re = flow->Re; s->Pr = flow->Pr; s->dt = dt;
+  Geo& g = s->g;
+  g.N1 = N1; g.N2 = N2; g.N3 = N3; g.nrun = nrun;
+  g.dim3 = N2 > 1 ? 1 : 0;
+  g.K1 = N1 / 3;
+  g.Ky = g.dim3 ? N2 / 3 : 1;
+  g.K2 = g.dim3 ? 2 * (N2 / 3) - 1 : 1;
+  g.P = g.K1 * g.K2;
+  g.Pp = (g.P + 15) / 16 * 16;
+  g.logN1 = ilog2(N1);
+  g.logN2 = ilog2(N2);
+  g.inv_n12 = 1.0f / (float)(N1 * N2);
+  g.fblk = (long long)N3 * g.Pp;
+  g.mblk = (long long)N3 * N2 * g.K1;
+
+  auto cleanup_fail = [&](int code) { free_all(s); delete s; return code; };
+#define CKC(call)                                                                                  \
+  do {                                                                                             \
+    cudaError_t e__ = (call);                                                                      \
+    if (e__ != cudaSuccess) {                                                                      \
+      fail(e__ == cudaErrorMemoryAllocation ? SF_ENOMEM : SF_ECUDA,                                \
+           std::string(#call) + ": " + cudaGetErrorString(e__));                                   \
+      return cleanup_fail(e__ == cudaErrorMemoryAllocation ? SF_ENOMEM : SF_ECUDA);                \
+    }                                                                                              \
+  } while (0)
+
+  if (prepare_kernels() != 0) return cleanup_fail(fail(SF_ECUDA, "cudaFuncSetAttribute failed"));
+  CKC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  const size_t cb = sizeof(float2);
+  CKC(cudaMalloc(&s->S[0], cb * nrun * 5 * g.fblk));
+  CKC(cudaMalloc(&s->S[1], cb * nrun * 5 * g.fblk));
+  CKC(cudaMalloc(&s->rold, cb * nrun * 4 * g.fblk));
+  CKC(cudaMalloc(&s->rnl, cb * nrun * 4 * g.fblk));
+  CKC(cudaMalloc(&s->qbuf, cb * nrun * g.fblk));
+  CKC(cudaMemset(s->S[0], 0, cb * nrun * 5 * g.fblk));
+  CKC(cudaMemset(s->S[1], 0, cb * nrun * 5 * g.fblk));
+  CKC(cudaMemset(s->rold, 0, cb * nrun * 4 * g.fblk));
+  CKC(cudaMemset(s->rnl, 0, cb * nrun * 4 * g.fblk));
+  CKC(cudaMemset(s->qbuf, 0, cb * nrun * g.fblk));
+  if (g.dim3) {
+    CKC(cudaMalloc(&s->mixin, cb * nrun * 4 * g.mblk));
+    CKC(cudaMalloc(&s->mixout, cb * nrun * 8 * g.mblk));
+  }
+  CKC(cudaMalloc(&s->zc, sizeof(float) * ZC_COUNT * N3));
+  CKC(cudaMalloc(&s->fa, sizeof(float) * kNumFS * N3));
+  CKC(cudaMalloc(&s->fc, sizeof(float) * kNumFS * N3));
+  CKC(cudaMalloc(&s->inv_den, sizeof(float) * kNumFS * g.fblk));
+  CKC(cudaMalloc(&s->kx, sizeof(float) * g.K1));
+  CKC(cudaMalloc(&s->ky, sizeof(float) * g.K2));
+  CKC(cudaMalloc(&s->kxd, sizeof(double) * g.K1));
+  CKC(cudaMalloc(&s->kyd, sizeof(double) * g.K2));
+  CKC(cudaMalloc(&s->bands, sizeof(double) * 6 * N3));
+  CKC(cudaMalloc(&s->Ri, sizeof(float) * nrun));
+  CKC(cudaMalloc(&s->Ubar, sizeof(float) * nrun * N3));
+  CKC(cudaMalloc(&s->dBdz, sizeof(float) * nrun * N3));
+  CKC(cudaMalloc(&s->red, sizeof(double) * 4 * nrun));
+  CKC(cudaMalloc(&s->tw, sizeof(float2) * kMaxN / 2));
+  CKC(cudaMalloc(&s->stage_ref, sizeof(float2) * (size_t)(N1 / 2 + 1) * N2 * N3));
+
+  // ---- vertical grid, Field.cpp:3-83, in FP64 ----
+  const int N = N3;
+  std::vector<double> z(N, 0.0), zf(N, 0.0), DY(N, 0.0), DYF(N, 0.0);
+  {
+    const double cs = 2.0, L = flow->L3;
+    const double step = 2.0 / (double)(N - 2);   // Eigen LinSpaced(N-1,-1,1)
+    for (int i = 0; i < N - 1; i++) {
+      double x = (i == N - 2) ? 1.0 : -1.0 + i * step;
+      z[i + 1] = L * (cs * std::pow(x, 7) + x) / (cs + 1);
+    }
+    double off = (z[1] + z[2]) / 2;
+    for (int i = 1; i < N; i++) z[i] *= -L / off;
+    for (int i = 1; i <= N - 2; i++) zf[i] = 0.5 * (z[i] + z[i + 1]);
+    zf[0] = 2 * zf[1] - zf[2];
+    zf[N - 1] = 2 * zf[N - 2] - zf[N - 3];
+    for (int i = 1; i < N; i++) DY[i] = zf[i] - zf[i - 1];
+    for (int i = 1; i <= N - 2; i++) DYF[i] = z[i + 1] - z[i];
+    DYF[N - 1] = DYF[N - 2];
+    DYF[0] = DYF[1];
+  }
+  s->zN = z;
+  s->zfN = zf;
+  // ---- bands, Differentiation.cpp:6-110 ----
+  std::vector<double> b6(6 * (size_t)N, 0.0);   // d2n lo,di,up ; d2d lo,di,up
+  std::vector<float> zc((size_t)ZC_COUNT * N, 0.f);
+  for (int j = 1; j < N - 1; j++) {
+    b6[0 * N + j] = 1 / DY[j] / DYF[j];
+    b6[1 * N + j] = -1 / DY[j] / DYF[j] - 1 / DY[j + 1] / DYF[j];
+    b6[2 * N + j] = 1 / DY[j + 1] / DYF[j];
+  }
+  for (int j = 2; j < N - 1; j++) {
+    b6[3 * N + j] = 1 / DYF[j - 1] / DY[j];
+    b6[4 * N + j] = -1 / DYF[j - 1] / DY[j] - 1 / DYF[j] / DY[j];
+    b6[5 * N + j] = 1 / DYF[j] / DY[j];
+  }
+  for (int b = 0; b < 6; b++)
+    for (int j = 0; j < N; j++) zc[(size_t)(ZC_D2N_LO + b) * N + j] = (float)b6[(size_t)b * N + j];
+  for (int j = 2; j <= N - 1; j++) {
+    zc[(size_t)ZC_DND_LO * N + j] = (float)(-1 / DY[j]);
+    zc[(size_t)ZC_DND_DI * N + j] = (float)(1 / DY[j]);
+  }
+  for (int j = 1; j <= N - 1; j++) {
+    zc[(size_t)ZC_DDN_DI * N + j] = (float)(-1 / DYF[j]);
+    if (j < N - 1) zc[(size_t)ZC_DDN_UP * N + j] = (float)(1 / DYF[j]);
+    zc[(size_t)ZC_FULL_LO * N + j] = (float)(DYF[j] / (2 * DY[j]));
+    zc[(size_t)ZC_FULL_DI * N + j] = (float)(DYF[j - 1] / (2 * DY[j]));
+    zc[(size_t)ZC_TILDE_LO * N + j] = (float)(DYF[j - 1] / (2 * DY[j]));
+    zc[(size_t)ZC_TILDE_DI * N + j] = (float)(DYF[j] / (2 * DY[j]));
+  }
+  for (int k = 1; k < N - 1; k++) zc[(size_t)ZC_WZN * N + k] = (float)(z[k + 1] - z[k]);
+  for (int k = 2; k < N - 1; k++) zc[(size_t)ZC_WZD * N + k] = (float)(zf[k] - zf[k - 1]);
+  CKC(cudaMemcpy(s->bands, b6.data(), sizeof(double) * 6 * N, cudaMemcpyHostToDevice));
+  CKC(cudaMemcpy(s->zc, zc.data(), sizeof(float) * zc.size(), cudaMemcpyHostToDevice));
+  // ---- Fourier wavenumbers, Differentiation.cpp:113-160 ----
+  {
+    const double pi = 3.141592653589793238462;
+    auto k1 = kint(N1), k2 = kint(N2);
+    std::vector<double> kxd(g.K1), kyd(g.K2);
+    std::vector<float> kxf(g.K1), kyf(g.K2);
+    for (int j = 0; j < g.K1; j++) kxd[j] = k1[j] * (2 * pi) / flow->L1;
+    for (int q = 0; q < g.K2; q++) {
+      if (!g.dim3) { kyd[q] = 0; continue; }
+      int n2 = q < g.Ky ? q : q + N2 - g.K2;
+      kyd[q] = k2[n2] * (2 * pi) / flow->L2;
+    }
+    for (int j = 0; j < g.K1; j++) kxf[j] = (float)kxd[j];
+    for (int q = 0; q < g.K2; q++) kyf[q] = (float)kyd[q];
+    CKC(cudaMemcpy(s->kxd, kxd.data(), sizeof(double) * g.K1, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->kyd, kyd.data(), sizeof(double) * g.K2, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->kx, kxf.data(), sizeof(float) * g.K1, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(s->ky, kyf.data(), sizeof(float) * g.K2, cudaMemcpyHostToDevice));
+  }
+  // ---- twiddles e^{-2 pi i k/kMaxN}, FP64 -> FP32 ----
+  {
+    std::vector<float2> tw(kMaxN / 2);
+    for (int k = 0; k < kMaxN / 2; k++) {
+      double a = -2.0 * 3.141592653589793238462 * k / kMaxN;
+      tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CKC(cudaMemcpy(s->tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
+  }
+  s->hRi.assign(nrun, 0.f);
+  CKC(cudaMemset(s->Ri, 0, sizeof(float) * nrun));
+  CKC(cudaMemset(s->Ubar, 0, sizeof(float) * nrun * N3));
+  {
+    std::vector<float> ones((size_t)nrun * N3, 1.f);
+    CKC(cudaMemcpy(s->dBdz, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
+  }
+  int rc = refactor(s);
+  if (rc != SF_OK) return cleanup_fail(rc);
+#undef CKC
+  *out = s;
+  return SF_OK;
+}
+
+int sf_destroy(sf_solver* s) {
+  if (!s) return SF_OK;
+  cudaSetDevice(s->device);
+  cudaStreamSynchronize(s->st);
+  free_all(s);
+  delete s;
+  return SF_OK;
+}
+
+int sf_set_dt(sf_solver* s, double dt) {
+  if (!s || !(dt > 0)) return fail(SF_EINVAL, "dt must be positive");
+  s->dt = dt;
+  return refactor(s);
+}
+
+int sf_set_ri(sf_solver* s, int run, double Ri) {
+  if (!s || run < 0 || run >= s->g.nrun) return fail(SF_EINVAL, "bad run");
+  s->hRi[run] = (float)Ri;
+  CK(cudaMemcpyAsync(s->Ri + run, &s->hRi[run], sizeof(float), cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_set_background(sf_solver* s, int run, const double* U, const double* dBdz) {
+  if (!s || run < 0 || run >= s->g.nrun || !U || !dBdz) return fail(SF_EINVAL, "bad argument");
+  const int N = s->g.N3;
+  std::vector<float> u(N), d(N);
+  for (int j = 0; j < N; j++) { u[j] = (float)U[j]; d[j] = (float)dBdz[j]; }
+  CK(cudaMemcpyAsync(s->Ubar + (size_t)run * N, u.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s->st));
+  CK(cudaMemcpyAsync(s->dBdz + (size_t)run * N, d.data(), sizeof(float) * N, cudaMemcpyHostToDevice, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+static size_t ref_elems(const sf_solver* s) { return (size_t)(s->g.N1 / 2 + 1) * s->g.N2 * s->g.N3; }
+
+int sf_set_field(sf_solver* s, int run, int field, const float* ref) {
+  if (!s || run < 0 || run >= s->g.nrun || field < 0 || field > 4 || !ref) return fail(SF_EINVAL, "bad argument");
+  CK(cudaMemcpyAsync(s->stage_ref, ref, sizeof(float2) * ref_elems(s), cudaMemcpyHostToDevice, s->st));
+  float2* dst = s->S[s->cur] + ((size_t)run * 5 + field) * s->g.fblk;
+  if (field == SF_U2 && !s->g.dim3) {
+    CK(cudaMemsetAsync(dst, 0, sizeof(float2) * s->g.fblk, s->st));   // CopyToSolver zeroes u2 in 2D
+  } else {
+    s->launches += launch_gather_ref(s->g, s->stage_ref, dst, s->st);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_get_field(sf_solver* s, int run, int field, float* ref) {
+  if (!s || run < 0 || run >= s->g.nrun || field < 0 || field > 4 || !ref) return fail(SF_EINVAL, "bad argument");
+  CK(cudaMemsetAsync(s->stage_ref, 0, sizeof(float2) * ref_elems(s), s->st));
+  const float2* src = s->S[s->cur] + ((size_t)run * 5 + field) * s->g.fblk;
+  s->launches += launch_scatter_ref(s->g, src, s->stage_ref, s->st);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ref, s->stage_ref, sizeof(float2) * ref_elems(s), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_set_state_kept(sf_solver* s, const float* host) {
+  if (!s || !host) return fail(SF_EINVAL, "bad argument");
+  CK(cudaMemcpyAsync(s->S[s->cur], host, sizeof(float2) * s->g.nrun * 5 * s->g.fblk, cudaMemcpyHostToDevice,
+                     s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_get_state_kept(sf_solver* s, float* host) {
+  if (!s || !host) return fail(SF_EINVAL, "bad argument");
+  CK(cudaMemcpyAsync(host, s->S[s->cur], sizeof(float2) * s->g.nrun * 5 * s->g.fblk, cudaMemcpyDeviceToHost,
+                     s->st));
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_state_device(sf_solver* s, void** dptr, size_t* bytes) {
+  if (!s || !dptr) return fail(SF_EINVAL, "bad argument");
+  *dptr = s->S[s->cur];
+  if (bytes) *bytes = sizeof(float2) * s->g.nrun * 5 * s->g.fblk;
+  return SF_OK;
+}
+
+int sf_set_state_device(sf_solver* s, const void* dptr) {
+  if (!s || !dptr) return fail(SF_EINVAL, "bad argument");
+  CK(cudaMemcpyAsync(s->S[s->cur], dptr, sizeof(float2) * s->g.nrun * 5 * s->g.fblk, cudaMemcpyDeviceToDevice,
+                     s->st));
+  return SF_OK;
+}
+
+int sf_remove_divergence(sf_solver* s, double pm) {
+  if (!s) return fail(SF_EINVAL, "null solver");
+  StageArgs a = stage_args(s, 0, s->cur, false);
+  a.Sn = s->S[s->cur];   // in place
+  a.pm = (float)pm;
+  s->launches += launch_project(a, s->st);
+  CK(cudaGetLastError());
+  return SF_OK;
+}
+
+int sf_prepare(sf_solver* s) {
+  // FilterAll is implicit (only kept modes are stored); RemoveDivergence(0)
+  return sf_remove_divergence(s, 0.0);
+}
+
+static int step_impl(sf_solver* s, int nsteps, bool linear) {
+  if (!s || nsteps < 0) return fail(SF_EINVAL, "bad argument");
+  if (linear && !s->base_set) return fail(SF_ESTATE, "sf_step_linear needs sf_set_base first");
+  for (int i = 0; i < nsteps; i++) {
+    int rc = ensure_graph(s, linear, s->cur);
+    if (rc != SF_OK) return rc;
+    CK(cudaGraphLaunch(s->graph[linear][s->cur], s->st));
+    s->launches += s->launches_per_step[linear];
+    s->cur = 1 - s->cur;
+  }
+  CK(cudaGetLastError());
+  return SF_OK;
+}
+
+int sf_step(sf_solver* s, int nsteps) { return step_impl(s, nsteps, false); }
+int sf_step_linear(sf_solver* s, int nsteps) { return step_impl(s, nsteps, true); }
+
+int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const float* u3, const float* b) {
+  if (!s || run < 0 || run >= s->g.nrun || !u1 || !u3 || !b) return fail(SF_EINVAL, "bad argument");
+  const Geo& g = s->g;
+  if (!s->base) {
+    CK(cudaMalloc(&s->base, sizeof(float) * (size_t)g.nrun * 4 * g.N3 * g.N2 * g.N1));
+    CK(cudaMemset(s->base, 0, sizeof(float) * (size_t)g.nrun * 4 * g.N3 * g.N2 * g.N1));
+    drop_graphs(s);   // graphs captured before hold a null base pointer
+  }
+  float* scratch = nullptr;
+  if (g.dim3) CK(cudaMalloc(&scratch, sizeof(float2) * g.mblk));
+  const float* src[4] = {u1, u2, u3, b};
+  for (int f = 0; f < 4; f++) {
+    float* dst = s->base + ((size_t)run * 4 + f) * g.N3 * g.N2 * g.N1;
+    if (f == 1 && (!g.dim3 || !u2)) {
+      CK(cudaMemsetAsync(dst, 0, sizeof(float) * (size_t)g.N3 * g.N2 * g.N1, s->st));
+      continue;
+    }
+    CK(cudaMemcpyAsync(s->stage_ref, src[f], sizeof(float2) * ref_elems(s), cudaMemcpyHostToDevice, s->st));
+    s->launches += launch_gather_ref(g, s->stage_ref, s->qbuf, s->st);
+    s->launches += launch_base_nodal(g, s->qbuf, f, dst, s->tw, scratch, s->st);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s->st));
+  if (scratch) cudaFree(scratch);
+  s->base_set = true;
+  return SF_OK;
+}
+
+int sf_energy(sf_solver* s, int run, double* ke, double* pe) {
+  if (!s || run < 0 || run >= s->g.nrun) return fail(SF_EINVAL, "bad argument");
+  const Geo& g = s->g;
+  CK(cudaMemsetAsync(s->red, 0, sizeof(double) * 4, s->st));
+  const float2* st = s->S[s->cur] + (size_t)run * 5 * g.fblk;
+  s->launches += launch_energy(g, st, st, 1, s->zc, s->Ri, s->red, s->st);
+  CK(cudaGetLastError());
+  double h[4];
+  CK(cudaMemcpyAsync(h, s->red, sizeof(h), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  // IMEXRK::KE / PE (IMEXRK.h:395-411)
+  double e = 0.5 * (h[0] + h[2]);
+  if (g.dim3) e += 0.5 * h[1];
+  if (ke) *ke = e;
+  if (pe) *pe = (double)s->hRi[run] * 0.5 * h[3];
+  return SF_OK;
+}
+
+int sf_dot(sf_solver* sa, int ra, sf_solver* sb, int rb, double* out) {
+  if (!sa || !sb || !out || ra < 0 || ra >= sa->g.nrun || rb < 0 || rb >= sb->g.nrun)
+    return fail(SF_EINVAL, "bad argument");
+  if (sa->g.N1 != sb->g.N1 || sa->g.N2 != sb->g.N2 || sa->g.N3 != sb->g.N3)
+    return fail(SF_EINVAL, "grids differ");
+  if (sb != sa) CK(cudaStreamSynchronize(sb->st));
+  const Geo& g = sa->g;
+  CK(cudaMemsetAsync(sa->red, 0, sizeof(double) * 4, sa->st));
+  const float2* A = sa->S[sa->cur] + (size_t)ra * 5 * g.fblk;
+  const float2* B = sb->S[sb->cur] + (size_t)rb * 5 * g.fblk;
+  sa->launches += launch_energy(g, A, B, 1, sa->zc, sa->Ri, sa->red, sa->st);
+  CK(cudaGetLastError());
+  double h[4];
+  CK(cudaMemcpyAsync(h, sa->red, sizeof(h), cudaMemcpyDeviceToHost, sa->st));
+  CK(cudaStreamSynchronize(sa->st));
+  // StateVector::Dot (StateVector.h:122-134)
+  double d = h[0] + h[2] + (double)sa->hRi[ra] * h[3];
+  if (g.dim3) d += h[1];
+  *out = d;
+  return SF_OK;
+}
+
+int sf_profile_step(sf_solver* s, int nsteps, int linear, int cap, double* ms, int* nslots) {
+  if (!s || nsteps < 1 || !ms || !nslots) return fail(SF_EINVAL, "bad argument");
+  if (linear && !s->base_set) return fail(SF_ESTATE, "linear profile needs sf_set_base first");
+  const int per = stage_kernel_count(s->g), n = 3 * per;
+  if (cap < n) return fail(SF_EINVAL, "ms buffer too small");
+  std::vector<cudaEvent_t> ev(n + 1);
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  std::vector<double> acc(n, 0.0);
+  for (int it = 0; it < nsteps; it++) {
+    CK(cudaEventRecord(ev[0], s->st));
+    for (int k = 0; k < 3; k++) {
+      StageArgs a = stage_args(s, k, s->cur, linear != 0);
+      s->launches += launch_stage(a, s->st, &ev[1 + k * per]);
+      s->cur = 1 - s->cur;
+    }
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(ev[n]));
+    for (int i = 0; i < n; i++) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+      acc[i] += t;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int i = 0; i < n; i++) ms[i] = acc[i] / nsteps;
+  *nslots = n;
+  return SF_OK;
+}
+
+int sf_profile_names(sf_solver* s, char* buf, size_t len) {
+  if (!s || !buf || len == 0) return fail(SF_EINVAL, "bad argument");
+  std::string out;
+  for (int k = 0; k < 3; k++)
+    for (int i = 0; i < stage_kernel_count(s->g); i++) {
+      if (!out.empty()) out += ",";
+      out += stage_kernel_name(s->g, i);
+    }
+  if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
+  std::memcpy(buf, out.c_str(), out.size() + 1);
+  return SF_OK;
+}
+
+int sf_synchronize(sf_solver* s) {
+  if (!s) return fail(SF_EINVAL, "null solver");
+  CK(cudaStreamSynchronize(s->st));
+  return SF_OK;
+}
+
+int sf_stream(sf_solver* s, void** stream) {
+  if (!s || !stream) return fail(SF_EINVAL, "bad argument");
+  *stream = (void*)s->st;
+  return SF_OK;
+}
+
+int sf_launch_count(sf_solver* s, long long* count) {
+  if (!s || !count) return fail(SF_EINVAL, "bad argument");
+  *count = s->launches;
+  return SF_OK;
+}
+
+}  // extern "C"
