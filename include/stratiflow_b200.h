@@ -144,6 +144,22 @@ int sf_profile_step(sf_solver* s, int nsteps, int linear, int cap, double* ms, i
 /* comma-separated kernel names of the profile slots */
 int sf_profile_names(sf_solver* s, char* buf, size_t len);
 
+/* RemoveDivergence(pressure_multiplier) for callers that cannot allocate
+ * device memory (no counterpart in the reference). It projects one run's
+ * fields that the caller owns on the device, in the kept layout
+ * [N3][plane]: u1, u2 (3D only; may be NULL in 2D) and u3 are updated in
+ * place, p_out = p_in + pressure_multiplier * q (p_out may equal p_in).
+ * It calls no allocator: its working memory is a fixed 2 MiB device array
+ * inside this library, which limits it to N3 * plane <= 131072 and
+ * N3 <= 1024 (larger grids return SF_EINVAL). The first call on a device
+ * looks that array up (cudaGetSymbolAddress), so make it before any stream
+ * capture. Work is queued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns without waiting. All calls share the array:
+ * calls whose GPU work overlaps race and must be serialised by the caller. */
+int sf_remove_divergence_noalloc(const sf_grid* grid, const sf_flow* flow, double pressure_multiplier,
+                                 void* u1, void* u2, void* u3, const void* p_in, void* p_out,
+                                 void* stream);
+
 /* waits for all work queued on the solver's stream */
 int sf_synchronize(sf_solver* s);
 

@@ -29,7 +29,7 @@ EXPORTS = [
     "sf_set_field", "sf_get_field", "sf_set_state_kept", "sf_get_state_kept", "sf_state_device",
     "sf_set_state_device", "sf_prepare", "sf_remove_divergence", "sf_step", "sf_set_base",
     "sf_step_linear", "sf_energy", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
-    "sf_profile_step", "sf_profile_names",
+    "sf_profile_step", "sf_profile_names", "sf_remove_divergence_noalloc",
 ]
 
 
@@ -71,6 +71,7 @@ def load_library(path: str | None = None):
         "sf_energy": [vp, i, dp, dp], "sf_dot": [vp, i, vp, i, dp], "sf_synchronize": [vp],
         "sf_stream": [vp, C.POINTER(vp)], "sf_launch_count": [vp, C.POINTER(C.c_longlong)],
         "sf_profile_step": [vp, i, i, i, dp, C.POINTER(i)], "sf_profile_names": [vp, C.c_char_p, C.c_size_t],
+        "sf_remove_divergence_noalloc": [C.POINTER(_Grid), C.POINTER(_Flow), d, vp, vp, vp, vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -15,6 +15,9 @@ using namespace sf;
 
 static thread_local std::string g_err;
 
+// used by the other translation units of the library
+void sf_set_error_message(const std::string& msg) { g_err = msg; }
+
 static int fail(int code, const std::string& msg) {
   g_err = msg;
   return code;
