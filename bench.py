@@ -286,6 +286,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="shear3d", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="warm up, then print the per-kernel times of --steps eager steps (for ncu)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     wl = WORKLOADS[args.config]
@@ -302,6 +304,13 @@ def main():
     import torch
     torch.cuda.set_device(local)
     s = make_solver(wl, local, seed=2024 + rank)
+    if args.profile_only:
+        s.TimeStep(args.warmup)
+        s.synchronize()
+        for name, t in s.profile_step(nsteps=max(1, args.steps)):
+            print(f"{name} {t:.4f} ms")
+        s.synchronize()
+        return
     stream = torch.cuda.ExternalStream(s.stream(), device=torch.device("cuda", local))
 
     # warm-up (also captures the step graph)

@@ -64,7 +64,7 @@ struct StageArgs {
   const float* Ri;      // nrun
   const float* Ubar;    // nrun x N3
   const float* dBdz;    // nrun x N3
-  const float2* tw;     // kMaxN/2 twiddles e^{-2 pi i k/kMaxN}
+  const float2* tw;     // kMaxN twiddles e^{-2 pi i k/kMaxN}, the full circle
   const float* base;    // nrun x 4 x N3 x N2 x N1 (linear step only)
   int stage;
   int linear;
@@ -102,7 +102,7 @@ __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y
 
 // In-place radix-2 decimation-in-time FFT of n = 2^logn points held in shared
 // memory at a[0..n), executed by one warp. Unnormalised; sign -1 (forward)
-// or +1 (inverse). tw holds e^{-2 pi i k/kMaxN} for k < kMaxN/2.
+// or +1 (inverse). tw holds e^{-2 pi i k/kMaxN}, k < kMaxN (only k < kMaxN/2 used here).
 __device__ __forceinline__ void warp_fft(float2* a, int n, int logn, const float2* __restrict__ tw,
                                          bool inverse, int lane) {
   const int shift = 32 - logn;

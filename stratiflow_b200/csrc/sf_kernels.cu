@@ -14,74 +14,84 @@
 // ModalField arithmetic touches (Field.h:1129-1166).
 
 #include "sf_internal.cuh"
+#include "sf_fft.cuh"
 
 namespace sf {
 
 // ===================================================== y transforms (3D) ====
-constexpr int kCG = 16;          // kx columns per block in the y transforms
 constexpr int kYThreads = 128;
 
 __device__ __forceinline__ int n2_of_q(int q, int Ky, int K2, int N2) { return q < Ky ? q : q + N2 - K2; }
 
-// modal [q][j1] of (run, field f, level j) -> mixed [y][j1], inverse c2c in y
+// kx columns handled by one block of the y transforms: one per lane group
+template <int N2>
+__host__ __device__ constexpr int ycols() { return (kYThreads / 32) * (32 / FFTShape<N2>::G); }
+
+// modal [q][j1] of (run, field f, level j) -> mixed [y][j1], inverse c2c in y.
+// One lane group per kx column; consecutive columns in consecutive groups so
+// that a warp's loads of one y row cover whole 32-byte sectors.
+template <int N2>
 __global__ void __launch_bounds__(kYThreads) k_ifft_y(StageArgs a) {
+  constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E, BUF = fft_buf_stride<N2>();
   const Geo g = a.g;
-  extern __shared__ float2 smem[];
-  const int ld = g.N2 + 1;
-  const int cg0 = blockIdx.x * kCG;
+  __shared__ float2 fbuf[(kYThreads / G) * BUF];
+  const int lane = threadIdx.x & 31, grp = threadIdx.x / G, l = threadIdx.x % G;
+  const int j1 = blockIdx.x * ycols<N2>() + grp;
   const int j = blockIdx.y;
   const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
+  const bool act = j1 < g.K1;
   const float2* src = a.S + ((size_t)(run * 5 + f) * g.N3 + j) * g.Pp;
-  for (int i = threadIdx.x; i < kCG * ld; i += blockDim.x) smem[i] = make_float2(0.f, 0.f);
-  __syncthreads();
-  for (int i = threadIdx.x; i < g.K2 * kCG; i += blockDim.x) {
-    int q = i / kCG, c = i - q * kCG, j1 = cg0 + c;
-    if (j1 < g.K1) smem[c * ld + n2_of_q(q, g.Ky, g.K2, g.N2)] = src[q * g.K1 + j1];
+  float2 x[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int n2 = l + G * e;
+    // kept rows: ky = 0..Ky-1 at n2 < Ky, ky = -(Ky-1)..-1 at n2 > N2 - Ky
+    int q = -1;
+    if (n2 < g.Ky) q = n2;
+    else if (n2 > N2 - g.Ky) q = n2 - (N2 - g.K2);
+    x[e] = (act && q >= 0) ? src[q * g.K1 + j1] : make_float2(0.f, 0.f);
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int c = warp; c < kCG; c += nw)
-    if (cg0 + c < g.K1) warp_fft(smem + c * ld, g.N2, g.logN2, a.tw, true, lane);
-  __syncthreads();
-  float2* dst = a.mixin + ((size_t)(run * 4 + f) * g.N3 + j) * g.N2 * g.K1;
-  for (int i = threadIdx.x; i < g.N2 * kCG; i += blockDim.x) {
-    int y = i / kCG, c = i - y * kCG, j1 = cg0 + c;
-    if (j1 < g.K1) dst[(size_t)y * g.K1 + j1] = smem[c * ld + y];
+  (void)lane;
+  reg_fft<N2, true>(x, fbuf + (threadIdx.x / G) * BUF, a.tw, l);
+  if (act) {
+    float2* dst = a.mixin + ((size_t)(run * 4 + f) * g.N3 + j) * N2 * g.K1 + j1;
+#pragma unroll
+    for (int sl = 0; sl < E; sl++) dst[(size_t)reg_fft_out_index<N2>(l, sl) * g.K1] = x[sl];
   }
 }
 
 // mixed combos (C_f, C_fy) [y][j1] -> r_f[q][j1] = Fy(C_f) + i ky Fy(C_fy)
+template <int N2>
 __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
+  constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E, BUF = fft_buf_stride<N2>();
   const Geo g = a.g;
-  extern __shared__ float2 smem[];
-  const int ld = g.N2 + 1;
-  const int cg0 = blockIdx.x * kCG;
+  __shared__ float2 fbuf[(kYThreads / G) * BUF];
+  const int grp = threadIdx.x / G, l = threadIdx.x % G;
+  const int j1 = blockIdx.x * ycols<N2>() + grp;
   const int j = blockIdx.y;
   const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
-  const float2* cA = a.mixout + ((size_t)(run * 8 + 2 * f) * g.N3 + j) * g.N2 * g.K1;
-  const float2* cB = a.mixout + ((size_t)(run * 8 + 2 * f + 1) * g.N3 + j) * g.N2 * g.K1;
-  for (int i = threadIdx.x; i < g.N2 * kCG; i += blockDim.x) {
-    int y = i / kCG, c = i - y * kCG, j1 = cg0 + c;
-    float2 va = make_float2(0.f, 0.f), vb = va;
-    if (j1 < g.K1) {
-      va = cA[(size_t)y * g.K1 + j1];
-      vb = cB[(size_t)y * g.K1 + j1];
-    }
-    smem[c * ld + y] = va;
-    smem[(kCG + c) * ld + y] = vb;
+  const bool act = j1 < g.K1;
+  const float2* cA = a.mixout + ((size_t)(run * 8 + 2 * f) * g.N3 + j) * N2 * g.K1 + j1;
+  const float2* cB = a.mixout + ((size_t)(run * 8 + 2 * f + 1) * g.N3 + j) * N2 * g.K1 + j1;
+  float2 xa[E], xb[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const size_t o = (size_t)(l + G * e) * g.K1;
+    xa[e] = act ? cA[o] : make_float2(0.f, 0.f);
+    xb[e] = act ? cB[o] : make_float2(0.f, 0.f);
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int c = warp; c < 2 * kCG; c += nw)
-    if (cg0 + (c % kCG) < g.K1) warp_fft(smem + c * ld, g.N2, g.logN2, a.tw, false, lane);
-  __syncthreads();
-  float2* dst = a.rnl + ((size_t)(run * 4 + f) * g.N3 + j) * g.Pp;
-  for (int i = threadIdx.x; i < g.K2 * kCG; i += blockDim.x) {
-    int q = i / kCG, c = i - q * kCG, j1 = cg0 + c;
-    if (j1 < g.K1) {
-      int n2 = n2_of_q(q, g.Ky, g.K2, g.N2);
-      float2 v = cadd(smem[c * ld + n2], cik(a.ky[q], smem[(kCG + c) * ld + n2]));
-      dst[q * g.K1 + j1] = v;
+  float2* buf = fbuf + grp * BUF;
+  reg_fft<N2, false>(xa, buf, a.tw, l);
+  reg_fft<N2, false>(xb, buf, a.tw, l);
+  if (act) {
+    float2* dst = a.rnl + ((size_t)(run * 4 + f) * g.N3 + j) * g.Pp + j1;
+#pragma unroll
+    for (int sl = 0; sl < E; sl++) {
+      const int n2 = reg_fft_out_index<N2>(l, sl);
+      int q = -1;
+      if (n2 < g.Ky) q = n2;
+      else if (n2 > N2 - g.Ky) q = n2 - (N2 - g.K2);
+      if (q >= 0) dst[(size_t)q * g.K1] = cadd(xa[sl], cik(a.ky[q], xb[sl]));
     }
   }
 }
@@ -95,16 +105,16 @@ constexpr int kXWarps = kXThreads / 32;
 
 struct XLayout {  // shared-memory carve-up of k_xpass
   int S, N1, K1, nprod;
-  size_t hat_off, work_off, nod_off, base_off, bytes;
+  size_t hat_off, buf_off, nod_off, base_off, bytes;
 };
 
-__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear) {
+__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int G) {
   XLayout L;
   L.S = S; L.N1 = N1; L.K1 = K1;
   L.nprod = dim3 ? P_COUNT : 6;
   size_t off = 0;
   L.hat_off = off;  off += sizeof(float2) * (size_t)L.nprod * (S + 2) * K1;
-  L.work_off = off; off += sizeof(float2) * (size_t)kXWarps * N1;
+  L.buf_off = off;  off += sizeof(float2) * (size_t)(kXThreads / G) * bufstride;
   L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.bytes = off;
@@ -119,71 +129,141 @@ __device__ __forceinline__ void prod_slots(int p, int S, int& first, int& count)
   else { first = 1; count = S; }
 }
 
-template <int S, bool LINEAR>
-__global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a) {
+// value of product p at slot s (level t) and x position x
+template <bool LINEAR>
+__device__ __forceinline__ float prod_value(int p, int s, int t, int x, const float* nod, const float* bnod, int NS,
+                                            int N1, int N3, const float* Ub, const float* zc) {
+  auto nr = [&](int f, int ss) { return nod[((size_t)f * NS + ss) * N1 + x]; };
+  auto br = [&](int f, int ss) { return bnod[((size_t)f * NS + ss) * N1 + x]; };
+  const float u1 = nr(0, s), u2 = nr(1, s), u3 = nr(2, s), bb = nr(3, s);
+  const float ub = Ub[t];
+  const bool lo = (t >= 1) && (s >= 1);   // rows with a level below (Bar, Tilde rows j >= 1)
+  const float tlo = zc[ZC_TILDE_LO * N3 + t], tdi = zc[ZC_TILDE_DI * N3 + t];
+  if (!LINEAR) {
+    const float U1t = u1 + ub;
+    switch (p) {
+      // U1t*U1t enters only through ddx (IMEXRK.cpp:155-156); its x-independent
+      // U_^2 part lies in the kx = 0 mode, which ddx multiplies by zero, so it
+      // is left out of the product to keep the FP32 rounding small
+      case P_S1: return u1 * (2.f * ub + u1);
+      case P_SB1: return U1t * bb;
+      case P_P3: return lo ? (tlo * (nr(0, s - 1) + Ub[t - 1]) + tdi * U1t) * u3 : 0.f;
+      case P_Q1: return lo ? (0.5f * (nr(0, s - 1) + Ub[t - 1]) + 0.5f * U1t) * u3 : 0.f;
+      case P_QB: return lo ? (0.5f * nr(3, s - 1) + 0.5f * bb) * u3 : 0.f;
+      case P_P4: {
+        const float d = (t <= N3 - 2) ? 0.5f * u3 + 0.5f * nr(2, s + 1) : 0.5f * u3;
+        return d * d;
+      }
+      case P_S12: return U1t * u2;
+      case P_S22: return u2 * u2;
+      case P_SB2: return u2 * bb;
+      case P_Q2: return lo ? (0.5f * nr(1, s - 1) + 0.5f * u2) * u3 : 0.f;
+      case P_P3Y: return lo ? (tlo * nr(1, s - 1) + tdi * u2) * u3 : 0.f;
+    }
+    return 0.f;
+  } else {
+    const float nn = br(0, s), u2b = br(1, s), u3b = br(2, s), bbb = br(3, s);
+    switch (p) {
+      case P_S1: return 2.f * (u1 * nn);
+      case P_SB1: return bb * nn + bbb * u1;
+      case P_P3: return lo ? (tlo * nr(0, s - 1) + tdi * u1) * u3b + (tlo * br(0, s - 1) + tdi * nn) * u3 : 0.f;
+      case P_Q1: return lo ? (0.5f * nr(0, s - 1) + 0.5f * u1) * u3b + (0.5f * br(0, s - 1) + 0.5f * nn) * u3 : 0.f;
+      case P_QB: return lo ? (0.5f * nr(3, s - 1) + 0.5f * bb) * u3b + (0.5f * br(3, s - 1) + 0.5f * bbb) * u3 : 0.f;
+      case P_P4: {
+        float d, db;
+        if (t <= N3 - 2) {
+          d = 0.5f * u3 + 0.5f * nr(2, s + 1);
+          db = 0.5f * u3b + 0.5f * br(2, s + 1);
+        } else {
+          d = 0.5f * u3;
+          db = 0.5f * u3b;
+        }
+        return 2.f * (d * db);
+      }
+      case P_S12: return u1 * u2b + nn * u2;
+      case P_S22: return 2.f * (u2 * u2b);
+      case P_SB2: return bb * u2b + bbb * u2;
+      case P_Q2: return lo ? (0.5f * nr(1, s - 1) + 0.5f * u2) * u3b + (0.5f * br(1, s - 1) + 0.5f * u2b) * u3 : 0.f;
+      case P_P3Y: return lo ? (tlo * nr(1, s - 1) + tdi * u2) * u3b + (tlo * br(1, s - 1) + tdi * u2b) * u3 : 0.f;
+    }
+    return 0.f;
+  }
+}
+
+// One block per (slab of S output levels, y row, run). Lane groups of G
+// lanes each run one transform at a time; all groups of the block step
+// through their task lists in lockstep so every lane reaches every warp sync.
+template <int N1, bool LINEAR>
+__global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a, int S) {
+  constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, BUF = fft_buf_stride<N1>();
+  constexpr int NGB = kXThreads / G;   // lane groups per block
   const Geo g = a.g;
   extern __shared__ __align__(16) unsigned char xsm[];
-  const XLayout L = x_layout(S, g.N1, g.K1, g.dim3, LINEAR);
+  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, G);
   float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
-  float2* work = reinterpret_cast<float2*>(xsm + L.work_off);
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
-  const int N1 = g.N1, K1 = g.K1, N3 = g.N3;
+  const int K1 = g.K1, N3 = g.N3;
   const int j0 = blockIdx.x * S;
   const int y = blockIdx.y;
   const int run = blockIdx.z;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gid = threadIdx.x / G, l = threadIdx.x % G;
+  float2* buf = reinterpret_cast<float2*>(xsm + L.buf_off) + (size_t)gid * BUF;
   const float* Ub = a.Ubar + (size_t)run * N3;
   const float* zc = a.zc;
-  float2* wk = work + (size_t)warp * N1;
   const int NS = S + 2;
 
-  auto nrow = [&](int f, int s) -> float* { return nod + ((size_t)f * NS + s) * N1; };
-  auto brow = [&](int f, int s) -> float* { return bnod + ((size_t)f * NS + s) * N1; };
-
-  // ---- phase A: inverse transforms of u1,u3 and b,u2 in pairs (ToNodal) ----
-  const int npairs = g.dim3 ? 2 : 2;
-  for (int task = warp; task < NS * npairs; task += kXWarps) {
-    const int s = task / npairs, pr = task - s * npairs;
+  // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
+  const int ntA = NS * 2;
+  for (int base = 0; base < ntA; base += NGB) {
+    const int task = base + gid;
+    const bool valid = task < ntA;
+    const int s = valid ? task >> 1 : 0, pr = task & 1;
     const int t = j0 - 1 + s;
+    const bool live = valid && t >= 0 && t < N3;
     const int fA = pr == 0 ? 0 : 3;       // u1 | b
     const int fB = pr == 0 ? 2 : 1;       // u3 | u2
-    float* rA = nrow(pr == 0 ? 0 : 3, s);
-    float* rB = nrow(pr == 0 ? 2 : 1, s);
-    if (t < 0 || t >= N3) {
-      for (int x = lane; x < N1; x += 32) { rA[x] = 0.f; rB[x] = 0.f; }
-      continue;
-    }
     const bool hasB = (fB != 1) || g.dim3;
     const float2* srcA;
     const float2* srcB;
     if (g.dim3) {
-      srcA = a.mixin + (((size_t)(run * 4 + fA) * N3 + t) * g.N2 + y) * K1;
-      srcB = a.mixin + (((size_t)(run * 4 + fB) * N3 + t) * g.N2 + y) * K1;
+      srcA = a.mixin + (((size_t)(run * 4 + fA) * N3 + (live ? t : 0)) * g.N2 + y) * K1;
+      srcB = a.mixin + (((size_t)(run * 4 + fB) * N3 + (live ? t : 0)) * g.N2 + y) * K1;
     } else {
-      srcA = a.S + ((size_t)(run * 5 + fA) * N3 + t) * g.Pp;
-      srcB = a.S + ((size_t)(run * 5 + fB) * N3 + t) * g.Pp;
+      srcA = a.S + ((size_t)(run * 5 + fA) * N3 + (live ? t : 0)) * g.Pp;
+      srcB = a.S + ((size_t)(run * 5 + fB) * N3 + (live ? t : 0)) * g.Pp;
     }
-    for (int x = lane; x < N1; x += 32) wk[x] = make_float2(0.f, 0.f);
-    __syncwarp();
-    for (int k = lane; k < K1; k += 32) {
-      float2 A = srcA[k];
-      float2 B = hasB ? srcB[k] : make_float2(0.f, 0.f);
-      if (k == 0) {
-        wk[0] = make_float2(A.x, B.x);  // c2r uses the real part of the k = 0 term
-      } else {
-        wk[k] = make_float2(A.x - B.y, A.y + B.x);        // A + iB
-        wk[N1 - k] = make_float2(A.x + B.y, B.x - A.y);   // conj(A) + i conj(B)
+    float2 x[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int n = l + G * e;
+      float2 z = make_float2(0.f, 0.f);
+      if (live) {
+        if (n == 0) {
+          // c2r uses the real part of the k = 0 term
+          z = make_float2(srcA[0].x, hasB ? srcB[0].x : 0.f);
+        } else if (n < K1) {
+          const float2 A = srcA[n], B = hasB ? srcB[n] : make_float2(0.f, 0.f);
+          z = make_float2(A.x - B.y, A.y + B.x);            // A + iB
+        } else if (n > N1 - K1) {
+          const int k = N1 - n;
+          const float2 A = srcA[k], B = hasB ? srcB[k] : make_float2(0.f, 0.f);
+          z = make_float2(A.x + B.y, B.x - A.y);            // conj(A) + i conj(B)
+        }
+      }
+      x[e] = z;
+    }
+    reg_fft<N1, true>(x, buf, a.tw, l);
+    if (valid) {
+      float* rA = nod + ((size_t)(pr == 0 ? 0 : 3) * NS + s) * N1;
+      float* rB = nod + ((size_t)(pr == 0 ? 2 : 1) * NS + s) * N1;
+#pragma unroll
+      for (int sl = 0; sl < E; sl++) {
+        const int xo = reg_fft_out_index<N1>(l, sl);
+        rA[xo] = x[sl].x;
+        rB[xo] = x[sl].y;
       }
     }
-    __syncwarp();
-    warp_fft(wk, N1, g.logN1, a.tw, true, lane);
-    for (int x = lane; x < N1; x += 32) {
-      float2 v = wk[x];
-      rA[x] = v.x;
-      rB[x] = v.y;
-    }
-    __syncwarp();
   }
   if (LINEAR) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
     for (int i = threadIdx.x; i < 4 * NS * N1; i += kXThreads) {
@@ -203,102 +283,48 @@ __global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a) {
   const int nprod = L.nprod;
   int nrows = 0;
   for (int p = 0; p < nprod; p++) { int f0, c; prod_slots(p, S, f0, c); nrows += c; }
-  const int ntask = (nrows + 1) / 2;
-  for (int task = warp; task < ntask; task += kXWarps) {
-    int pp[2], ss[2];
+  const int ntB = (nrows + 1) / 2;
+  const float sc = 0.5f * g.inv_n12;
+  for (int base = 0; base < ntB; base += NGB) {
+    const int task = base + gid;
+    int pp[2], ss[2], tt[2];
     bool live[2];
+#pragma unroll
     for (int h = 0; h < 2; h++) {
       int r = 2 * task + h;
-      pp[h] = -1; ss[h] = 0; live[h] = false;
-      if (r < nrows) {
+      pp[h] = -1; ss[h] = 0; tt[h] = 0; live[h] = false;
+      if (task < ntB && r < nrows) {
         for (int p = 0; p < nprod; p++) {
           int f0, c; prod_slots(p, S, f0, c);
           if (r < c) { pp[h] = p; ss[h] = f0 + r; break; }
           r -= c;
         }
-        int t = j0 - 1 + ss[h];
-        live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
+        tt[h] = j0 - 1 + ss[h];
+        live[h] = (pp[h] >= 0) && tt[h] >= 0 && tt[h] < N3;
       }
     }
-    for (int x = lane; x < N1; x += 32) {
-      float v[2];
-      for (int h = 0; h < 2; h++) {
-        v[h] = 0.f;
-        if (!live[h]) continue;
-        const int s = ss[h], t = j0 - 1 + s;
-        const float u1 = nrow(0, s)[x], u2 = nrow(1, s)[x], u3 = nrow(2, s)[x], bb = nrow(3, s)[x];
-        const float ub = Ub[t];
-        const bool lo = (t >= 1) && (s >= 1);   // rows with a level below (Bar, Tilde rows j >= 1)
-        const float u1m = lo ? nrow(0, s - 1)[x] : 0.f;
-        const float u2m = lo ? nrow(1, s - 1)[x] : 0.f;
-        const float bm = lo ? nrow(3, s - 1)[x] : 0.f;
-        const float ubm = lo ? Ub[t - 1] : 0.f;
-        const float tlo = zc[ZC_TILDE_LO * N3 + t], tdi = zc[ZC_TILDE_DI * N3 + t];
-        if (!LINEAR) {
-          const float U1t = u1 + ub, U1tm = u1m + ubm;
-          switch (pp[h]) {
-            // U1t*U1t enters only through ddx (IMEXRK.cpp:155-156); the x-independent
-            // U_^2 part lies in the kx = 0 mode, which ddx multiplies by zero, so
-            // it is left out of the product to keep the FP32 rounding small.
-            case P_S1: v[h] = u1 * (2.f * ub + u1); break;
-            case P_SB1: v[h] = U1t * bb; break;
-            case P_P3: v[h] = lo ? (tlo * U1tm + tdi * U1t) * u3 : 0.f; break;
-            case P_Q1: v[h] = lo ? (0.5f * U1tm + 0.5f * U1t) * u3 : 0.f; break;
-            case P_QB: v[h] = lo ? (0.5f * bm + 0.5f * bb) * u3 : 0.f; break;
-            case P_P4: {
-              float d = (t <= N3 - 2) ? 0.5f * u3 + 0.5f * nrow(2, s + 1)[x] : 0.5f * u3;
-              v[h] = d * d;
-            } break;
-            case P_S12: v[h] = U1t * u2; break;
-            case P_S22: v[h] = u2 * u2; break;
-            case P_SB2: v[h] = u2 * bb; break;
-            case P_Q2: v[h] = lo ? (0.5f * u2m + 0.5f * u2) * u3 : 0.f; break;
-            case P_P3Y: v[h] = lo ? (tlo * u2m + tdi * u2) * u3 : 0.f; break;
-          }
-        } else {
-          const float nn = brow(0, s)[x], u2b = brow(1, s)[x], u3b = brow(2, s)[x], bbb = brow(3, s)[x];
-          const float nnm = lo ? brow(0, s - 1)[x] : 0.f;
-          const float u2bm = lo ? brow(1, s - 1)[x] : 0.f;
-          const float bbm = lo ? brow(3, s - 1)[x] : 0.f;
-          switch (pp[h]) {
-            case P_S1: v[h] = 2.f * (u1 * nn); break;
-            case P_SB1: v[h] = bb * nn + bbb * u1; break;
-            case P_P3: v[h] = lo ? (tlo * u1m + tdi * u1) * u3b + (tlo * nnm + tdi * nn) * u3 : 0.f; break;
-            case P_Q1: v[h] = lo ? (0.5f * u1m + 0.5f * u1) * u3b + (0.5f * nnm + 0.5f * nn) * u3 : 0.f; break;
-            case P_QB: v[h] = lo ? (0.5f * bm + 0.5f * bb) * u3b + (0.5f * bbm + 0.5f * bbb) * u3 : 0.f; break;
-            case P_P4: {
-              float d, db;
-              if (t <= N3 - 2) {
-                d = 0.5f * u3 + 0.5f * nrow(2, s + 1)[x];
-                db = 0.5f * u3b + 0.5f * brow(2, s + 1)[x];
-              } else {
-                d = 0.5f * u3;
-                db = 0.5f * u3b;
-              }
-              v[h] = 2.f * (d * db);
-            } break;
-            case P_S12: v[h] = u1 * u2b + nn * u2; break;
-            case P_S22: v[h] = 2.f * (u2 * u2b); break;
-            case P_SB2: v[h] = bb * u2b + bbb * u2; break;
-            case P_Q2: v[h] = lo ? (0.5f * u2m + 0.5f * u2) * u3b + (0.5f * u2bm + 0.5f * u2b) * u3 : 0.f; break;
-            case P_P3Y: v[h] = lo ? (tlo * u2m + tdi * u2) * u3b + (tlo * u2bm + tdi * u2b) * u3 : 0.f; break;
-          }
-        }
-      }
-      wk[x] = make_float2(v[0], v[1]);
+    float2 x[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int n = l + G * e;
+      const float v0 = live[0] ? prod_value<LINEAR>(pp[0], ss[0], tt[0], n, nod, bnod, NS, N1, N3, Ub, zc) : 0.f;
+      const float v1 = live[1] ? prod_value<LINEAR>(pp[1], ss[1], tt[1], n, nod, bnod, NS, N1, N3, Ub, zc) : 0.f;
+      x[e] = make_float2(v0, v1);
     }
+    reg_fft<N1, false>(x, buf, a.tw, l);
+    // natural order in the group's buffer, then split the two real transforms
+#pragma unroll
+    for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
     __syncwarp();
-    warp_fft(wk, N1, g.logN1, a.tw, false, lane);
-    const float sc = 0.5f * g.inv_n12;
-    for (int k = lane; k < K1; k += 32) {
-      float2 zk = wk[k];
-      float2 zc2 = cconj(wk[(N1 - k) & (N1 - 1)]);
+    for (int k = l; k < K1; k += G) {
+      const float2 zk = buf[k];
+      const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
       if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
-        hat[((size_t)pp[0] * NS + ss[0]) * K1 + k] = live[0] ? make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc)
-                                                             : make_float2(0.f, 0.f);
+        hat[((size_t)pp[0] * NS + ss[0]) * K1 + k] =
+            live[0] ? make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc) : make_float2(0.f, 0.f);
       if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
-        hat[((size_t)pp[1] * NS + ss[1]) * K1 + k] = live[1] ? make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc)
-                                                             : make_float2(0.f, 0.f);
+        hat[((size_t)pp[1] * NS + ss[1]) * K1 + k] =
+            live[1] ? make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc) : make_float2(0.f, 0.f);
     }
     __syncwarp();
   }
@@ -717,24 +743,66 @@ __global__ void k_inner(Geo g, const float2* __restrict__ Sa, const float2* __re
 // ======================================================== launchers ====
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
-static int launch_xpass(const StageArgs& a, cudaStream_t st) {
+template <int N1, bool LIN>
+static void xpass_launch(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
-  // slab of output levels per block: the largest of 8, 4, 2 whose shared
-  // memory fits in one SM's opt-in limit
-  int S = 8;
-  for (; S > 2; S >>= 1)
-    if (x_layout(S, g.N1, g.K1, g.dim3, a.linear).bytes <= 200 * 1024) break;
+  constexpr int G = FFTShape<N1>::G, BUF = fft_buf_stride<N1>();
+  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, G).bytes; };
+  // largest slab whose shared memory lets two blocks share an SM, then
+  // smaller slabs while the grid would leave SMs idle
+  const int cand[] = {8, 6, 4, 3, 2};
+  int S = 2;
+  for (int c : cand)
+    if (bytes(c) <= 112 * 1024) { S = c; break; }
+  if (bytes(S) > 112 * 1024) S = 2;
   if (g.dim3 && S > 4) S = 4;
-  size_t sm = x_layout(S, g.N1, g.K1, g.dim3, a.linear).bytes;
-  dim3 grid(cdiv(g.N3, S), g.N2, g.nrun);
-#define XCASE(SV, LIN) k_xpass<SV, LIN><<<grid, kXThreads, sm, st>>>(a);
-  if (a.linear) {
-    if (S == 8) XCASE(8, true) else if (S == 4) XCASE(4, true) else XCASE(2, true)
-  } else {
-    if (S == 8) XCASE(8, false) else if (S == 4) XCASE(4, false) else XCASE(2, false)
+  for (int i = 0; i < 5; i++) {
+    if (cand[i] >= S) continue;
+    if ((long long)((g.N3 + S - 1) / S) * g.N2 * g.nrun >= 2 * 148) break;
+    S = cand[i];
   }
-#undef XCASE
+  dim3 grid(cdiv(g.N3, S), g.N2, g.nrun);
+  k_xpass<N1, LIN><<<grid, kXThreads, bytes(S), st>>>(a, S);
+}
+
+static int launch_xpass(const StageArgs& a, cudaStream_t st) {
+  const bool L = a.linear != 0;
+  switch (a.g.N1) {
+    case 16: L ? xpass_launch<16, true>(a, st) : xpass_launch<16, false>(a, st); break;
+    case 32: L ? xpass_launch<32, true>(a, st) : xpass_launch<32, false>(a, st); break;
+    case 64: L ? xpass_launch<64, true>(a, st) : xpass_launch<64, false>(a, st); break;
+    case 128: L ? xpass_launch<128, true>(a, st) : xpass_launch<128, false>(a, st); break;
+    case 256: L ? xpass_launch<256, true>(a, st) : xpass_launch<256, false>(a, st); break;
+    case 512: L ? xpass_launch<512, true>(a, st) : xpass_launch<512, false>(a, st); break;
+  }
   return 1;
+}
+
+template <int N2>
+static void ify_launch(const StageArgs& a, int nrun, cudaStream_t st) {
+  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, nrun * 4), kYThreads, 0, st>>>(a);
+}
+template <int N2>
+static void fy_launch(const StageArgs& a, cudaStream_t st) {
+  k_fft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, a.g.nrun * 4), kYThreads, 0, st>>>(a);
+}
+static void launch_ifft_y(const StageArgs& a, int nrun, cudaStream_t st) {
+  switch (a.g.N2) {
+    case 16: ify_launch<16>(a, nrun, st); break;
+    case 32: ify_launch<32>(a, nrun, st); break;
+    case 64: ify_launch<64>(a, nrun, st); break;
+    case 128: ify_launch<128>(a, nrun, st); break;
+    case 256: ify_launch<256>(a, nrun, st); break;
+  }
+}
+static void launch_fft_y(const StageArgs& a, cudaStream_t st) {
+  switch (a.g.N2) {
+    case 16: fy_launch<16>(a, st); break;
+    case 32: fy_launch<32>(a, st); break;
+    case 64: fy_launch<64>(a, st); break;
+    case 128: fy_launch<128>(a, st); break;
+    case 256: fy_launch<256>(a, st); break;
+  }
 }
 
 // opt-in shared-memory limits of every kernel, set once per process before
@@ -743,9 +811,10 @@ int prepare_kernels() {
   const int lim = 227 * 1024;
   cudaError_t e = cudaSuccess;
 #define ATTR(K) if (e == cudaSuccess) e = cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  ATTR(k_ifft_y) ATTR(k_fft_y)
-  ATTR((k_xpass<8, false>)) ATTR((k_xpass<4, false>)) ATTR((k_xpass<2, false>))
-  ATTR((k_xpass<8, true>)) ATTR((k_xpass<4, true>)) ATTR((k_xpass<2, true>))
+  ATTR((k_xpass<16, false>)) ATTR((k_xpass<32, false>)) ATTR((k_xpass<64, false>))
+  ATTR((k_xpass<128, false>)) ATTR((k_xpass<256, false>)) ATTR((k_xpass<512, false>))
+  ATTR((k_xpass<16, true>)) ATTR((k_xpass<32, true>)) ATTR((k_xpass<64, true>))
+  ATTR((k_xpass<128, true>)) ATTR((k_xpass<256, true>)) ATTR((k_xpass<512, true>))
 #undef ATTR
   return e == cudaSuccess ? 0 : -1;
 }
@@ -773,15 +842,13 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     n++;
   };
   if (g.dim3) {
-    size_t sm = sizeof(float2) * kCG * (g.N2 + 1);
-    k_ifft_y<<<dim3(cdiv(g.K1, kCG), g.N3, g.nrun * 4), kYThreads, sm, st>>>(a);
+    launch_ifft_y(a, g.nrun, st);
     mark();
   }
   launch_xpass(a, st);
   mark();
   if (g.dim3) {
-    size_t sm = sizeof(float2) * 2 * kCG * (g.N2 + 1);
-    k_fft_y<<<dim3(cdiv(g.K1, kCG), g.N3, g.nrun * 4), kYThreads, sm, st>>>(a);
+    launch_fft_y(a, st);
     mark();
   }
   k_z_cn<<<dim3(cdiv(2 * g.P, kZThreads), g.dim3 ? 4 : 3, g.nrun), kZThreads, 0, st>>>(a);
@@ -850,8 +917,7 @@ int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* 
   a.S = kept_modal;   // treated as field 0 of a one-run state
   a.mixin = reinterpret_cast<float2*>(scratch_mixed);
   a.tw = tw;
-  size_t sm = sizeof(float2) * kCG * (g.N2 + 1);
-  k_ifft_y<<<dim3(cdiv(g.K1, kCG), g.N3, 1), kYThreads, sm, st>>>(a);
+  launch_ifft_y(a, 1, st);
   k_base_x<<<dim3(g.N3, g.N2), 32, sizeof(float2) * g.N1, st>>>(g, a.mixin, (long long)g.N2 * g.K1, g.K1,
                                                                 base_out, tw);
   return 2;

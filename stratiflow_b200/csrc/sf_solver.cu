@@ -278,7 +278,7 @@ int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, s
   CKC(cudaMalloc(&s->Ubar, sizeof(float) * nrun * N3));
   CKC(cudaMalloc(&s->dBdz, sizeof(float) * nrun * N3));
   CKC(cudaMalloc(&s->red, sizeof(double) * 4 * nrun));
-  CKC(cudaMalloc(&s->tw, sizeof(float2) * kMaxN / 2));
+  CKC(cudaMalloc(&s->tw, sizeof(float2) * kMaxN));
   CKC(cudaMalloc(&s->stage_ref, sizeof(float2) * (size_t)(N1 / 2 + 1) * N2 * N3));
 
   // ---- vertical grid, Field.cpp:3-83, in FP64 ----
@@ -355,8 +355,8 @@ int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, s
   }
   // ---- twiddles e^{-2 pi i k/kMaxN}, FP64 -> FP32 ----
   {
-    std::vector<float2> tw(kMaxN / 2);
-    for (int k = 0; k < kMaxN / 2; k++) {
+    std::vector<float2> tw(kMaxN);
+    for (int k = 0; k < kMaxN; k++) {
       double a = -2.0 * 3.141592653589793238462 * k / kMaxN;
       tw[k] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
