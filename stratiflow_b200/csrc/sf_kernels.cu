@@ -100,107 +100,174 @@ __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
 // product ids (BuildRHS, IMEXRK.cpp:155-192; BuildRHSLinear, :212-257)
 enum Prod { P_S1, P_SB1, P_P3, P_Q1, P_QB, P_P4, P_S12, P_S22, P_SB2, P_Q2, P_P3Y, P_COUNT };
 
-constexpr int kXThreads = 256;
-constexpr int kXWarps = kXThreads / 32;
+constexpr int kXMaxThreads = 512;
+
+// slots s = 0..S+1 hold level j0-1+s; product p is formed at slots
+// [first, first+count)
+__host__ __device__ __forceinline__ void prod_slots(int p, int S, int& first, int& count) {
+  if (p == P_Q1 || p == P_QB || p == P_Q2) { first = 1; count = S + 1; }
+  else if (p == P_P4) { first = 0; count = S + 1; }
+  else { first = 1; count = S; }
+}
+__host__ __device__ inline int prod_rows(int nprod, int S) {
+  int n = 0;
+  for (int p = 0; p < nprod; p++) { int f, c; prod_slots(p, S, f, c); n += c; }
+  return n;
+}
+
+// row of the transformed product p at slot s; p is a compile-time constant at
+// every call, so the loop folds
+__device__ __forceinline__ int hat_row(int p, int s, int S) {
+  int base = 0;
+#pragma unroll
+  for (int q = 0; q < P_COUNT; q++) {
+    if (q == p) break;
+    int f, c;
+    prod_slots(q, S, f, c);
+    base += c;
+  }
+  int f, c;
+  prod_slots(p, S, f, c);
+  return base + s - f;
+}
 
 struct XLayout {  // shared-memory carve-up of k_xpass
-  int S, N1, K1, nprod;
+  int nprod, nrows;
   size_t hat_off, buf_off, nod_off, base_off, bytes;
 };
 
-__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int G) {
+__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int ngroups) {
   XLayout L;
-  L.S = S; L.N1 = N1; L.K1 = K1;
   L.nprod = dim3 ? P_COUNT : 6;
+  L.nrows = prod_rows(L.nprod, S);
   size_t off = 0;
-  L.hat_off = off;  off += sizeof(float2) * (size_t)L.nprod * (S + 2) * K1;
-  L.buf_off = off;  off += sizeof(float2) * (size_t)(kXThreads / G) * bufstride;
+  // transformed products, one row of K1 per (product, slot); before phase B
+  // the same bytes stage the input rows of phase A (4 x (S+2) x K1)
+  size_t hat = sizeof(float2) * (size_t)L.nrows * K1, stage = sizeof(float2) * (size_t)4 * (S + 2) * K1;
+  L.hat_off = off;  off += (hat > stage ? hat : stage);
+  L.buf_off = off;  off += sizeof(float2) * (size_t)ngroups * bufstride;
   L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.bytes = off;
   return L;
 }
 
-// slots s = 0..S+1 hold level j0-1+s; product p is formed at slots
-// [first, first+count)
-__device__ __forceinline__ void prod_slots(int p, int S, int& first, int& count) {
-  if (p == P_Q1 || p == P_QB || p == P_Q2) { first = 1; count = S + 1; }
-  else if (p == P_P4) { first = 0; count = S + 1; }
-  else { first = 1; count = S; }
+// One term (a0 F[s] + a1 F[s-1] + a2)(b0 G[s] + b1 G[s+1] + b2) of a product:
+// every product of BuildRHS is one such term and every product of
+// BuildRHSLinear the sum of two.
+struct PTerm {
+  const float *F, *Fm, *Gs, *Gp;
+  float a0, a1, a2, b0, b1, b2;
+};
+
+__device__ __forceinline__ void term_set(PTerm& T, const float* F, const float* Fm, float a0, float a1, float a2,
+                                         const float* Gs, const float* Gp, float b0, float b1, float b2) {
+  T.F = F; T.Fm = Fm; T.a0 = a0; T.a1 = a1; T.a2 = a2;
+  T.Gs = Gs; T.Gp = Gp; T.b0 = b0; T.b1 = b1; T.b2 = b2;
 }
 
-// value of product p at slot s (level t) and x position x
+// the terms of product p at slot s (level t); rows of the nodal fields
+// U1,U2,U3,B (`nr`) and of the frozen base (`br`: U1b+U_, U2b, U3b, Bb)
 template <bool LINEAR>
-__device__ __forceinline__ float prod_value(int p, int s, int t, int x, const float* nod, const float* bnod, int NS,
-                                            int N1, int N3, const float* Ub, const float* zc) {
-  auto nr = [&](int f, int ss) { return nod[((size_t)f * NS + ss) * N1 + x]; };
-  auto br = [&](int f, int ss) { return bnod[((size_t)f * NS + ss) * N1 + x]; };
-  const float u1 = nr(0, s), u2 = nr(1, s), u3 = nr(2, s), bb = nr(3, s);
-  const float ub = Ub[t];
-  const bool lo = (t >= 1) && (s >= 1);   // rows with a level below (Bar, Tilde rows j >= 1)
-  const float tlo = zc[ZC_TILDE_LO * N3 + t], tdi = zc[ZC_TILDE_DI * N3 + t];
+__device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, int NS, const float* nod,
+                                           const float* bnod, const float* Ub, const float* zc, PTerm& T0,
+                                           PTerm& T1) {
+  auto nr = [&](int f, int ss) { return nod + ((size_t)f * NS + ss) * N1; };
+  auto br = [&](int f, int ss) { return bnod + ((size_t)f * NS + ss) * N1; };
+  const bool lo = (t >= 1) && (s >= 1);    // Bar/Tilde rows j >= 1 have a level below
+  const int sm = lo ? s - 1 : s;
+  const float top = (t <= N3 - 2) ? 1.f : 0.f;   // ReinterpolateDirichlet's last row
+  const int sp = (t <= N3 - 2) ? s + 1 : s;
+  const float lof = lo ? 1.f : 0.f;
+  const float tlo = lof * zc[ZC_TILDE_LO * N3 + t], tdi = lof * zc[ZC_TILDE_DI * N3 + t];
+  const float hb = 0.5f * lof;
+  const float ub = Ub[t], ubm = lo ? Ub[t - 1] : 0.f;
+  const float* z = nr(0, s);   // any valid row for unused pointers
+  term_set(T1, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
   if (!LINEAR) {
-    const float U1t = u1 + ub;
     switch (p) {
       // U1t*U1t enters only through ddx (IMEXRK.cpp:155-156); its x-independent
       // U_^2 part lies in the kx = 0 mode, which ddx multiplies by zero, so it
       // is left out of the product to keep the FP32 rounding small
-      case P_S1: return u1 * (2.f * ub + u1);
-      case P_SB1: return U1t * bb;
-      case P_P3: return lo ? (tlo * (nr(0, s - 1) + Ub[t - 1]) + tdi * U1t) * u3 : 0.f;
-      case P_Q1: return lo ? (0.5f * (nr(0, s - 1) + Ub[t - 1]) + 0.5f * U1t) * u3 : 0.f;
-      case P_QB: return lo ? (0.5f * nr(3, s - 1) + 0.5f * bb) * u3 : 0.f;
-      case P_P4: {
-        const float d = (t <= N3 - 2) ? 0.5f * u3 + 0.5f * nr(2, s + 1) : 0.5f * u3;
-        return d * d;
-      }
-      case P_S12: return U1t * u2;
-      case P_S22: return u2 * u2;
-      case P_SB2: return u2 * bb;
-      case P_Q2: return lo ? (0.5f * nr(1, s - 1) + 0.5f * u2) * u3 : 0.f;
-      case P_P3Y: return lo ? (tlo * nr(1, s - 1) + tdi * u2) * u3 : 0.f;
+      case P_S1: term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 2.f * ub); break;
+      case P_SB1: term_set(T0, nr(0, s), z, 1.f, 0.f, ub, nr(3, s), z, 1.f, 0.f, 0.f); break;
+      case P_P3: term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, tlo * ubm + tdi * ub, nr(2, s), z, lof, 0.f, 0.f); break;
+      case P_Q1: term_set(T0, nr(0, s), nr(0, sm), hb, hb, hb * ubm + hb * ub, nr(2, s), z, lof, 0.f, 0.f); break;
+      case P_QB: term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
+      case P_P4: term_set(T0, nr(2, s), nr(2, sp), 0.5f, 0.5f * top, 0.f, nr(2, s), nr(2, sp), 0.5f, 0.5f * top, 0.f); break;
+      case P_S12: term_set(T0, nr(0, s), z, 1.f, 0.f, ub, nr(1, s), z, 1.f, 0.f, 0.f); break;
+      case P_S22: term_set(T0, nr(1, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f); break;
+      case P_SB2: term_set(T0, nr(1, s), z, 1.f, 0.f, 0.f, nr(3, s), z, 1.f, 0.f, 0.f); break;
+      case P_Q2: term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
+      case P_P3Y: term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
+      default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
     }
-    return 0.f;
   } else {
-    const float nn = br(0, s), u2b = br(1, s), u3b = br(2, s), bbb = br(3, s);
     switch (p) {
-      case P_S1: return 2.f * (u1 * nn);
-      case P_SB1: return bb * nn + bbb * u1;
-      case P_P3: return lo ? (tlo * nr(0, s - 1) + tdi * u1) * u3b + (tlo * br(0, s - 1) + tdi * nn) * u3 : 0.f;
-      case P_Q1: return lo ? (0.5f * nr(0, s - 1) + 0.5f * u1) * u3b + (0.5f * br(0, s - 1) + 0.5f * nn) * u3 : 0.f;
-      case P_QB: return lo ? (0.5f * nr(3, s - 1) + 0.5f * bb) * u3b + (0.5f * br(3, s - 1) + 0.5f * bbb) * u3 : 0.f;
-      case P_P4: {
-        float d, db;
-        if (t <= N3 - 2) {
-          d = 0.5f * u3 + 0.5f * nr(2, s + 1);
-          db = 0.5f * u3b + 0.5f * br(2, s + 1);
-        } else {
-          d = 0.5f * u3;
-          db = 0.5f * u3b;
-        }
-        return 2.f * (d * db);
-      }
-      case P_S12: return u1 * u2b + nn * u2;
-      case P_S22: return 2.f * (u2 * u2b);
-      case P_SB2: return bb * u2b + bbb * u2;
-      case P_Q2: return lo ? (0.5f * nr(1, s - 1) + 0.5f * u2) * u3b + (0.5f * br(1, s - 1) + 0.5f * u2b) * u3 : 0.f;
-      case P_P3Y: return lo ? (tlo * nr(1, s - 1) + tdi * u2) * u3b + (tlo * br(1, s - 1) + tdi * u2b) * u3 : 0.f;
+      case P_S1: term_set(T0, nr(0, s), z, 2.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f); break;
+      case P_SB1:
+        term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f);
+        term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 0.f);
+        break;
+      case P_P3:
+        term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
+        term_set(T1, br(0, s), br(0, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+        break;
+      case P_Q1:
+        term_set(T0, nr(0, s), nr(0, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+        term_set(T1, br(0, s), br(0, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+        break;
+      case P_QB:
+        term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+        term_set(T1, br(3, s), br(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+        break;
+      case P_P4:   // 2 Dir(U3) Dir(U3b)
+        term_set(T0, nr(2, s), nr(2, sp), 1.f, top, 0.f, br(2, s), br(2, sp), 0.5f, 0.5f * top, 0.f);
+        break;
+      case P_S12:
+        term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
+        term_set(T1, br(0, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
+        break;
+      case P_S22: term_set(T0, nr(1, s), z, 2.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f); break;
+      case P_SB2:
+        term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
+        term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
+        break;
+      case P_Q2:
+        term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+        term_set(T1, br(1, s), br(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+        break;
+      case P_P3Y:
+        term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
+        term_set(T1, br(1, s), br(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+        break;
+      default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
     }
-    return 0.f;
   }
 }
+
+__device__ __forceinline__ float term_eval(const PTerm& T, int x) {
+  return (T.a0 * T.F[x] + T.a1 * T.Fm[x] + T.a2) * (T.b0 * T.Gs[x] + T.b1 * T.Gp[x] + T.b2);
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
 // One block per (slab of S output levels, y row, run). Lane groups of G
 // lanes each run one transform at a time; all groups of the block step
 // through their task lists in lockstep so every lane reaches every warp sync.
 template <int N1, bool LINEAR>
-__global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a, int S) {
+__global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, BUF = fft_buf_stride<N1>();
-  constexpr int NGB = kXThreads / G;   // lane groups per block
+  const int NGB = blockDim.x / G;   // lane groups per block
   const Geo g = a.g;
   extern __shared__ __align__(16) unsigned char xsm[];
-  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, G);
+  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB);
   float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
+  float2* stg = hat;                                           // phase A input rows [4][S+2][K1]
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
   const int K1 = g.K1, N3 = g.N3;
@@ -212,61 +279,23 @@ __global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a, int S) {
   const float* Ub = a.Ubar + (size_t)run * N3;
   const float* zc = a.zc;
   const int NS = S + 2;
+  const int nf = g.dim3 ? 4 : 4;
 
-  // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
-  const int ntA = NS * 2;
-  for (int base = 0; base < ntA; base += NGB) {
-    const int task = base + gid;
-    const bool valid = task < ntA;
-    const int s = valid ? task >> 1 : 0, pr = task & 1;
+  // ---- stage the input rows (u1,u2,u3,b at levels j0-1 .. j0+S) ----
+  for (int i = threadIdx.x; i < nf * NS * K1; i += blockDim.x) {
+    const int f = i / (NS * K1), r = i - f * NS * K1, s = r / K1, k = r - s * K1;
     const int t = j0 - 1 + s;
-    const bool live = valid && t >= 0 && t < N3;
-    const int fA = pr == 0 ? 0 : 3;       // u1 | b
-    const int fB = pr == 0 ? 2 : 1;       // u3 | u2
-    const bool hasB = (fB != 1) || g.dim3;
-    const float2* srcA;
-    const float2* srcB;
-    if (g.dim3) {
-      srcA = a.mixin + (((size_t)(run * 4 + fA) * N3 + (live ? t : 0)) * g.N2 + y) * K1;
-      srcB = a.mixin + (((size_t)(run * 4 + fB) * N3 + (live ? t : 0)) * g.N2 + y) * K1;
+    float2* d = stg + i;
+    if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
+      *d = make_float2(0.f, 0.f);
+    } else if (g.dim3) {
+      cp_async8(d, a.mixin + (((size_t)(run * 4 + f) * N3 + t) * g.N2 + y) * K1 + k);
     } else {
-      srcA = a.S + ((size_t)(run * 5 + fA) * N3 + (live ? t : 0)) * g.Pp;
-      srcB = a.S + ((size_t)(run * 5 + fB) * N3 + (live ? t : 0)) * g.Pp;
-    }
-    float2 x[E];
-#pragma unroll
-    for (int e = 0; e < E; e++) {
-      const int n = l + G * e;
-      float2 z = make_float2(0.f, 0.f);
-      if (live) {
-        if (n == 0) {
-          // c2r uses the real part of the k = 0 term
-          z = make_float2(srcA[0].x, hasB ? srcB[0].x : 0.f);
-        } else if (n < K1) {
-          const float2 A = srcA[n], B = hasB ? srcB[n] : make_float2(0.f, 0.f);
-          z = make_float2(A.x - B.y, A.y + B.x);            // A + iB
-        } else if (n > N1 - K1) {
-          const int k = N1 - n;
-          const float2 A = srcA[k], B = hasB ? srcB[k] : make_float2(0.f, 0.f);
-          z = make_float2(A.x + B.y, B.x - A.y);            // conj(A) + i conj(B)
-        }
-      }
-      x[e] = z;
-    }
-    reg_fft<N1, true>(x, buf, a.tw, l);
-    if (valid) {
-      float* rA = nod + ((size_t)(pr == 0 ? 0 : 3) * NS + s) * N1;
-      float* rB = nod + ((size_t)(pr == 0 ? 2 : 1) * NS + s) * N1;
-#pragma unroll
-      for (int sl = 0; sl < E; sl++) {
-        const int xo = reg_fft_out_index<N1>(l, sl);
-        rA[xo] = x[sl].x;
-        rB[xo] = x[sl].y;
-      }
+      cp_async8(d, a.S + ((size_t)(run * 5 + f) * N3 + t) * g.Pp + k);
     }
   }
   if (LINEAR) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
-    for (int i = threadIdx.x; i < 4 * NS * N1; i += kXThreads) {
+    for (int i = threadIdx.x; i < 4 * NS * N1; i += blockDim.x) {
       int f = i / (NS * N1), r = i - f * NS * N1, s = r / N1, x = r - s * N1;
       int t = j0 - 1 + s;
       float v = 0.f;
@@ -277,38 +306,83 @@ __global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a, int S) {
       bnod[i] = v;
     }
   }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
+  const int ntA = NS * 2;
+  for (int base = 0; base < ntA; base += NGB) {
+    const int task = base + gid;
+    const bool valid = task < ntA;
+    const int s = valid ? task >> 1 : 0, pr = task & 1;
+    const int fA = pr == 0 ? 0 : 3;       // u1 | b
+    const int fB = pr == 0 ? 2 : 1;       // u3 | u2
+    const float2* srcA = stg + ((size_t)fA * NS + s) * K1;
+    const float2* srcB = stg + ((size_t)fB * NS + s) * K1;
+    float2 x[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int n = l + G * e;
+      float2 zz = make_float2(0.f, 0.f);
+      if (n == 0) {
+        zz = make_float2(srcA[0].x, srcB[0].x);   // c2r uses the real part of the k = 0 term
+      } else if (n < K1) {
+        const float2 A = srcA[n], B = srcB[n];
+        zz = make_float2(A.x - B.y, A.y + B.x);            // A + iB
+      } else if (n > N1 - K1) {
+        const float2 A = srcA[N1 - n], B = srcB[N1 - n];
+        zz = make_float2(A.x + B.y, B.x - A.y);            // conj(A) + i conj(B)
+      }
+      x[e] = zz;
+    }
+    reg_fft<N1, true>(x, buf, a.tw, l);
+    if (valid) {
+      float* rA = nod + ((size_t)fA * NS + s) * N1;
+      float* rB = nod + ((size_t)fB * NS + s) * N1;
+#pragma unroll
+      for (int sl = 0; sl < E; sl++) {
+        const int xo = reg_fft_out_index<N1>(l, sl);
+        rA[xo] = x[sl].x;
+        rB[xo] = x[sl].y;
+      }
+    }
+  }
   __syncthreads();
 
   // ---- phase B/C: nodal products, forward transforms in pairs (ToModal) ----
-  const int nprod = L.nprod;
-  int nrows = 0;
-  for (int p = 0; p < nprod; p++) { int f0, c; prod_slots(p, S, f0, c); nrows += c; }
+  const int nprod = L.nprod, nrows = L.nrows;
   const int ntB = (nrows + 1) / 2;
   const float sc = 0.5f * g.inv_n12;
   for (int base = 0; base < ntB; base += NGB) {
     const int task = base + gid;
-    int pp[2], ss[2], tt[2];
+    int pp[2], ss[2], row[2];
     bool live[2];
+    PTerm T[2][2];
 #pragma unroll
     for (int h = 0; h < 2; h++) {
       int r = 2 * task + h;
-      pp[h] = -1; ss[h] = 0; tt[h] = 0; live[h] = false;
+      pp[h] = -1; ss[h] = 0; live[h] = false; row[h] = r;
       if (task < ntB && r < nrows) {
         for (int p = 0; p < nprod; p++) {
           int f0, c; prod_slots(p, S, f0, c);
           if (r < c) { pp[h] = p; ss[h] = f0 + r; break; }
           r -= c;
         }
-        tt[h] = j0 - 1 + ss[h];
-        live[h] = (pp[h] >= 0) && tt[h] >= 0 && tt[h] < N3;
+        const int t = j0 - 1 + ss[h];
+        live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
       }
+      prod_terms<LINEAR>(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, nod, bnod, Ub, zc,
+                         T[h][0], T[h][1]);
     }
     float2 x[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int n = l + G * e;
-      const float v0 = live[0] ? prod_value<LINEAR>(pp[0], ss[0], tt[0], n, nod, bnod, NS, N1, N3, Ub, zc) : 0.f;
-      const float v1 = live[1] ? prod_value<LINEAR>(pp[1], ss[1], tt[1], n, nod, bnod, NS, N1, N3, Ub, zc) : 0.f;
+      float v0 = term_eval(T[0][0], n), v1 = term_eval(T[1][0], n);
+      if (LINEAR) {
+        v0 += term_eval(T[0][1], n);
+        v1 += term_eval(T[1][1], n);
+      }
       x[e] = make_float2(v0, v1);
     }
     reg_fft<N1, false>(x, buf, a.tw, l);
@@ -320,19 +394,17 @@ __global__ void __launch_bounds__(kXThreads) k_xpass(StageArgs a, int S) {
       const float2 zk = buf[k];
       const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
       if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
-        hat[((size_t)pp[0] * NS + ss[0]) * K1 + k] =
-            live[0] ? make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc) : make_float2(0.f, 0.f);
+        hat[(size_t)row[0] * K1 + k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);
       if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
-        hat[((size_t)pp[1] * NS + ss[1]) * K1 + k] =
-            live[1] ? make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc) : make_float2(0.f, 0.f);
+        hat[(size_t)row[1] * K1 + k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);
     }
     __syncwarp();
   }
   __syncthreads();
 
   // ---- phase D: z stencils of the products and x derivatives ----
-  auto H = [&](int p, int s, int k) -> float2 { return hat[((size_t)p * NS + s) * K1 + k]; };
-  for (int i = threadIdx.x; i < S * K1; i += kXThreads) {
+  auto H = [&](int p, int s, int k) -> float2 { return hat[(size_t)hat_row(p, s, S) * K1 + k]; };
+  for (int i = threadIdx.x; i < S * K1; i += blockDim.x) {
     const int si = i / K1, k = i - si * K1;
     const int t = j0 + si, s = si + 1;
     if (t >= N3) continue;
@@ -505,6 +577,299 @@ __global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
       x = bd[i] - (fc[j] * bi[i]) * x;
       out[2 * (size_t)j * Pp] = x;
     }
+  }
+}
+
+// ------------------------------------------------ chunked z solves ----
+// The Thomas sweeps are first-order affine recurrences: D_j = al_j D_{j-1} +
+// be_j (al_j = -a_j/den_j, be_j = R_j/den_j) upward, x_j = D_j - C_j x_{j+1}
+// downward. A block of kZW warps splits N3 into kZW z-chunks, one per warp,
+// and covers 16 modes x {real, imag} per warp: every chunk composes its
+// affine map, one warp scans the kZW maps in z order, and every chunk then
+// replays its levels from the right incoming value. be_j and D_j stay in
+// shared memory ([N3][32] floats per block). The result equals the sequential
+// sweep up to rounding.
+constexpr int kZW = 8;
+
+__device__ __forceinline__ void zscan_up(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
+  sA[w * 32 + lane] = A;
+  sB[w * 32 + lane] = B;
+  __syncthreads();
+  if (w == 0) {
+    float v = 0.f;
+    for (int k = 0; k < kZW; k++) {
+      sIn[k * 32 + lane] = v;
+      v = sA[k * 32 + lane] * v + sB[k * 32 + lane];
+    }
+  }
+  __syncthreads();
+}
+__device__ __forceinline__ void zscan_down(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
+  sA[w * 32 + lane] = A;
+  sB[w * 32 + lane] = B;
+  __syncthreads();
+  if (w == 0) {
+    float v = 0.f;
+    for (int k = kZW - 1; k >= 0; k--) {
+      sIn[k * 32 + lane] = v;
+      v = sA[k * 32 + lane] * v + sB[k * 32 + lane];
+    }
+  }
+  __syncthreads();
+}
+
+// k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
+// FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
+__global__ void __launch_bounds__(kZW * 32) k_z_cn_chunked(StageArgs a) {
+  const Geo g = a.g;
+  extern __shared__ float zsm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m0 = blockIdx.x * 16 + (lane >> 1), c = lane & 1;
+  const bool act = m0 < g.P;
+  const int m = act ? m0 : 0;
+  const int run = blockIdx.z;
+  const int fi = blockIdx.y;
+  const int f = g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
+  const int N3 = g.N3, Pp = g.Pp;
+  const int chunk = (N3 + kZW - 1) / kZW;
+  const int js = min(N3, w * chunk), je = min(N3, js + chunk);
+  float* sD = zsm;                      // [N3][32]: be_j, then D_j
+  float* sA = zsm + (size_t)N3 * 32;    // [kZW][32]
+  float* sB = sA + kZW * 32;
+  float* sIn = sB + kZW * 32;
+  const int q = m / g.K1, j1 = m - q * g.K1;
+  const float kxv = a.kx[j1], kyv = a.ky[q];
+  const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
+  const float sc = c == 0 ? -1.f : 1.f;   // (i k z)_c = sc * k * z_{1-c}
+  const bool dir = (f == 2);
+  const int fam = (f == 3) ? 1 : (dir ? 2 : 0);
+  const int fs = fam * 3 + a.stage;
+  const float* __restrict__ fa = a.fa + (size_t)fs * N3;
+  const float* __restrict__ fc = a.fc + (size_t)fs * N3;
+  const float* __restrict__ iden = a.inv_den + (size_t)fs * N3 * Pp + m;
+  const float* __restrict__ zc = a.zc;
+  const float* __restrict__ lo2 = zc + (dir ? ZC_D2D_LO : ZC_D2N_LO) * N3;
+  const float* __restrict__ di2 = zc + (dir ? ZC_D2D_DI : ZC_D2N_DI) * N3;
+  const float* __restrict__ up2 = zc + (dir ? ZC_D2D_UP : ZC_D2N_UP) * N3;
+  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
+  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
+  const float* __restrict__ full_lo = zc + ZC_FULL_LO * N3;
+  const float* __restrict__ full_di = zc + ZC_FULL_DI * N3;
+  const float cco = (f == 3) ? a.cb : a.cv;
+  const float Ri = a.Ri[run];
+  const float* __restrict__ dB = a.dBdz + (size_t)run * N3;
+  const bool zmode = (m == 0);   // the (0,0) mode: no buoyancy force (IMEXRK.cpp:141-143)
+  const size_t fo = (size_t)(run * 5 + f) * N3 * Pp + m;
+  const float* uc = reinterpret_cast<const float*>(a.S + fo) + c;
+  const float* pc = reinterpret_cast<const float*>(a.S + (size_t)(run * 5 + 4) * N3 * Pp + m) + c;
+  const float* po = reinterpret_cast<const float*>(a.S + (size_t)(run * 5 + 4) * N3 * Pp + m) + (1 - c);
+  const float* bc = reinterpret_cast<const float*>(a.S + (size_t)(run * 5 + 3) * N3 * Pp + m) + c;
+  const float* wc = reinterpret_cast<const float*>(a.S + (size_t)(run * 5 + 2) * N3 * Pp + m) + c;
+  const float* rc = reinterpret_cast<const float*>(a.rnl + (size_t)(run * 4 + f) * N3 * Pp + m) + c;
+  float* rold = reinterpret_cast<float*>(a.rold + (size_t)(run * 4 + f) * N3 * Pp + m) + c;
+  float* out = reinterpret_cast<float*>(a.Sn + fo) + c;
+  const bool use_rold = (a.hz != 0.f);
+  const float kgrad = (f == 0) ? kxv : kyv;
+  const size_t S2 = 2 * (size_t)Pp;
+
+  // ---- forward, pass 1: right-hand side, be_j, chunk map ----
+  float um = js >= 1 && js < N3 ? uc[(js - 1) * S2] : 0.f;
+  float u0 = js < N3 ? uc[js * S2] : 0.f;
+  float pm1 = (f == 2 && js >= 1 && js < N3) ? pc[(js - 1) * S2] : 0.f;
+  float bm1 = (f == 2 && js >= 1 && js < N3) ? bc[(js - 1) * S2] : 0.f;
+  float w0 = (f == 3 && js < N3) ? wc[js * S2] : 0.f;
+  float A = 1.f, B = 0.f;
+  for (int j0 = js; j0 < je; j0 += kZU) {
+    float bu[kZU], br[kZU], bo[kZU], bp[kZU], bx[kZU], bi[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      const bool in = j < je, nx = j + 1 < N3 && in;
+      bu[i] = nx ? uc[(j + 1) * S2] : 0.f;
+      br[i] = in ? rc[j * S2] : 0.f;
+      bo[i] = (in && use_rold) ? rold[j * S2] : 0.f;
+      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
+      bp[i] = 0.f;
+      bx[i] = 0.f;
+      if (f <= 1) bp[i] = in ? po[j * S2] : 0.f;
+      if (f == 2) {
+        bp[i] = in ? pc[j * S2] : 0.f;
+        bx[i] = in ? bc[j * S2] : 0.f;
+      }
+      if (f == 3) bx[i] = nx ? wc[(j + 1) * S2] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      if (j >= je) break;
+      const float up = bu[i];
+      float rt = br[i];
+      float gp = 0.f;
+      if (f <= 1) {
+        gp = sc * kgrad * bp[i];   // (i k p)_c
+      } else if (f == 2) {
+        if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
+        pm1 = bp[i];
+        if (j >= 1 && !zmode) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
+        bm1 = bx[i];
+      } else {
+        const float w1 = bx[i];
+        const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
+        rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
+        w0 = w1;
+      }
+      float R = u0;
+      if (use_rold) R += a.hz * bo[i];
+      R += -a.h * gp;
+      R += a.hb * rt;
+      const bool band = dir ? (j >= 2 && j <= N3 - 2) : (j >= 1 && j <= N3 - 2);
+      const float d2u = band ? lo2[j] * um + di2[j] * u0 + up2[j] * up : 0.f;
+      R += cco * ((d1 * u0 + d2 * u0) + d2u);
+      const bool zend = (j <= 1) || (j >= N3 - 2) || (dir && j == 2);   // ZeroEnds (Field.h:475-486)
+      if (zend) R = 0.f;
+      const float be = R * bi[i];
+      const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
+      sD[j * 32 + lane] = be;
+      if (act) rold[j * S2] = rt;
+      A = al * A;
+      B = al * B + be;
+      um = u0;
+      u0 = up;
+    }
+  }
+  zscan_up(sA, sB, sIn, w, lane, A, B);
+  // ---- forward, pass 2: D_j ----
+  float D = sIn[w * 32 + lane];
+  for (int j = js; j < je; j++) {
+    const float al = (j == 0) ? 0.f : -fa[j] * iden[(size_t)j * Pp];
+    D = al * D + sD[j * 32 + lane];
+    sD[j * 32 + lane] = D;
+  }
+  // ---- backward, pass 1: chunk map of x_j = D_j - C_j x_{j+1} ----
+  A = 1.f;
+  B = 0.f;
+  for (int j = je - 1; j >= js; j--) {
+    const float Cj = fc[j] * iden[(size_t)j * Pp];
+    A = -Cj * A;
+    B = -Cj * B + sD[j * 32 + lane];
+  }
+  __syncthreads();
+  zscan_down(sA, sB, sIn, w, lane, A, B);
+  // ---- backward, pass 2: the solution ----
+  float x = sIn[w * 32 + lane];
+  for (int j = je - 1; j >= js; j--) {
+    const float Cj = fc[j] * iden[(size_t)j * Pp];
+    x = sD[j * 32 + lane] - Cj * x;
+    if (act) out[j * S2] = x;
+  }
+}
+
+// RemoveDivergence with the chunked solve, for 16 modes per block: the
+// divergence and the Laplacian factors upward, q downward, then u -= grad q
+// and p += pm q. The two components of a mode are adjacent lanes and
+// exchange q; u3_{j+1} at a chunk's top uses the next chunk's q from the scan.
+__global__ void __launch_bounds__(kZW * 32) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
+                                                           const float* zc, const float* fa, const float* fc,
+                                                           const float* inv_den, const float* kx, const float* ky,
+                                                           float pm) {
+  extern __shared__ float zsm[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int m0 = blockIdx.x * 16 + (lane >> 1), c = lane & 1;
+  const bool act = m0 < g.P;
+  const int m = act ? m0 : 0;
+  const int run = blockIdx.z;
+  const int N3 = g.N3, Pp = g.Pp;
+  const int chunk = (N3 + kZW - 1) / kZW;
+  const int js = min(N3, w * chunk), je = min(N3, js + chunk);
+  float* sD = zsm;
+  float* sA = zsm + (size_t)N3 * 32;
+  float* sB = sA + kZW * 32;
+  float* sIn = sB + kZW * 32;
+  const int q = m / g.K1, j1 = m - q * g.K1;
+  const float kxv = kx[j1], kyv = g.dim3 ? ky[q] : 0.f;
+  const float sc = c == 0 ? -1.f : 1.f;
+  const size_t S2 = 2 * (size_t)Pp;
+  float* u1 = reinterpret_cast<float*>(U + (size_t)(run * 5 + 0) * N3 * Pp + m);
+  float* u2 = reinterpret_cast<float*>(U + (size_t)(run * 5 + 1) * N3 * Pp + m);
+  float* u3 = reinterpret_cast<float*>(U + (size_t)(run * 5 + 2) * N3 * Pp + m) + c;
+  const float* ps = reinterpret_cast<const float*>(Psrc + (size_t)(run * 5 + 4) * N3 * Pp + m) + c;
+  float* pd = reinterpret_cast<float*>(Pdst + (size_t)(run * 5 + 4) * N3 * Pp + m) + c;
+  const float* __restrict__ a_ = fa + (size_t)kFS_Lap * N3;
+  const float* __restrict__ c_ = fc + (size_t)kFS_Lap * N3;
+  const float* __restrict__ iden = inv_den + (size_t)kFS_Lap * N3 * Pp + m;
+  const float* __restrict__ ddn_di = zc + ZC_DDN_DI * N3;
+  const float* __restrict__ ddn_up = zc + ZC_DDN_UP * N3;
+  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
+  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
+  const float* u1o = u1 + (1 - c);   // u1_{1-c}
+  const float* u2o = u2 + (1 - c);
+  float* u1c = u1 + c;
+  float* u2c = u2 + c;
+
+  // ---- forward, pass 1: divergence, be_j, chunk map ----
+  float w0 = js < N3 ? u3[js * S2] : 0.f;
+  float A = 1.f, B = 0.f;
+  for (int j0 = js; j0 < je; j0 += kZU) {
+    float b1[kZU], b2[kZU], b3[kZU], bi[kZU];
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      const bool in = j < je;
+      b1[i] = in ? u1o[j * S2] : 0.f;
+      b2[i] = (in && g.dim3) ? u2o[j * S2] : 0.f;
+      b3[i] = (in && j + 1 < N3) ? u3[(j + 1) * S2] : 0.f;
+      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
+    }
+#pragma unroll
+    for (int i = 0; i < kZU; i++) {
+      const int j = j0 + i;
+      if (j >= je) break;
+      const float w1 = b3[i];
+      float dv = 0.f;
+      if (j >= 2 && j <= N3 - 3) dv = sc * (kxv * b1[i] + kyv * b2[i]) + (ddn_di[j] * w0 + ddn_up[j] * w1);
+      const float be = dv * bi[i];
+      const float al = (j == 0) ? 0.f : -a_[j] * bi[i];
+      sD[j * 32 + lane] = be;
+      A = al * A;
+      B = al * B + be;
+      w0 = w1;
+    }
+  }
+  zscan_up(sA, sB, sIn, w, lane, A, B);
+  float D = sIn[w * 32 + lane];
+  for (int j = js; j < je; j++) {
+    const float al = (j == 0) ? 0.f : -a_[j] * iden[(size_t)j * Pp];
+    D = al * D + sD[j * 32 + lane];
+    sD[j * 32 + lane] = D;
+  }
+  // ---- backward: q ----
+  auto Cof = [&](int j) {
+    float Cj = c_[j] * iden[(size_t)j * Pp];
+    if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
+    return Cj;
+  };
+  A = 1.f;
+  B = 0.f;
+  for (int j = je - 1; j >= js; j--) {
+    const float Cj = Cof(j);
+    A = -Cj * A;
+    B = -Cj * B + sD[j * 32 + lane];
+  }
+  __syncthreads();
+  zscan_down(sA, sB, sIn, w, lane, A, B);
+  // ---- backward, pass 2: q_j, projection, p ----
+  float qn = sIn[w * 32 + lane];   // q at level je (0 above the top)
+  for (int j = je - 1; j >= js; j--) {
+    const float qj = sD[j * 32 + lane] - Cof(j) * qn;
+    const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
+    if (act) {
+      u1c[j * S2] -= sc * kxv * qo;
+      if (g.dim3) u2c[j * S2] -= sc * kyv * qo;
+      pd[j * S2] = ps[j * S2] + pm * qj;
+      const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
+      if (jj >= 2 && jj <= N3 - 1) u3[jj * S2] -= dnd_lo[jj] * qj + dnd_di[jj] * qn;
+    }
+    qn = qj;
   }
 }
 
@@ -747,14 +1112,22 @@ template <int N1, bool LIN>
 static void xpass_launch(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
   constexpr int G = FFTShape<N1>::G, BUF = fft_buf_stride<N1>();
-  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, G).bytes; };
+  const int nprod = g.dim3 ? P_COUNT : 6;
+  // threads: enough lane groups for all phase-A transforms of a slab (one
+  // round), at least two warps, at most kXMaxThreads
+  auto threads = [&](int S) {
+    int groups = 2 * (S + 2);
+    int t = ((groups * G + 31) / 32) * 32;
+    return t < 64 ? 64 : (t > kXMaxThreads ? kXMaxThreads : t);
+  };
+  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, threads(S) / G).bytes; };
+  (void)nprod;
   // largest slab whose shared memory lets two blocks share an SM, then
   // smaller slabs while the grid would leave SMs idle
   const int cand[] = {8, 6, 4, 3, 2};
   int S = 2;
   for (int c : cand)
     if (bytes(c) <= 112 * 1024) { S = c; break; }
-  if (bytes(S) > 112 * 1024) S = 2;
   if (g.dim3 && S > 4) S = 4;
   for (int i = 0; i < 5; i++) {
     if (cand[i] >= S) continue;
@@ -762,7 +1135,7 @@ static void xpass_launch(const StageArgs& a, cudaStream_t st) {
     S = cand[i];
   }
   dim3 grid(cdiv(g.N3, S), g.N2, g.nrun);
-  k_xpass<N1, LIN><<<grid, kXThreads, bytes(S), st>>>(a, S);
+  k_xpass<N1, LIN><<<grid, threads(S), bytes(S), st>>>(a, S);
 }
 
 static int launch_xpass(const StageArgs& a, cudaStream_t st) {
@@ -815,15 +1188,17 @@ int prepare_kernels() {
   ATTR((k_xpass<128, false>)) ATTR((k_xpass<256, false>)) ATTR((k_xpass<512, false>))
   ATTR((k_xpass<16, true>)) ATTR((k_xpass<32, true>)) ATTR((k_xpass<64, true>))
   ATTR((k_xpass<128, true>)) ATTR((k_xpass<256, true>)) ATTR((k_xpass<512, true>))
+  ATTR(k_z_cn_chunked) ATTR(k_z_proj_chunked)
 #undef ATTR
   return e == cudaSuccess ? 0 : -1;
 }
 
+static size_t zchunk_smem(const Geo& g) { return sizeof(float) * ((size_t)g.N3 * 32 + 3 * kZW * 32); }
+
 int launch_project(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
-  dim3 grid(cdiv(2 * g.P, kZThreads), 1, g.nrun);
-  k_z_proj<<<grid, kZThreads, 0, st>>>(g, a.Sn, a.S, a.Sn, a.qbuf, a.zc, a.fa, a.fc, a.inv_den, a.kx, a.ky,
-                                       a.pm);
+  k_z_proj_chunked<<<dim3(cdiv(g.P, 16), 1, g.nrun), kZW * 32, zchunk_smem(g), st>>>(
+      g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc, a.inv_den, a.kx, a.ky, a.pm);
   return 1;
 }
 
@@ -851,7 +1226,7 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     launch_fft_y(a, st);
     mark();
   }
-  k_z_cn<<<dim3(cdiv(2 * g.P, kZThreads), g.dim3 ? 4 : 3, g.nrun), kZThreads, 0, st>>>(a);
+  k_z_cn_chunked<<<dim3(cdiv(g.P, 16), g.dim3 ? 4 : 3, g.nrun), kZW * 32, zchunk_smem(g), st>>>(a);
   mark();
   launch_project(a, st);
   mark();
