@@ -155,13 +155,14 @@ __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int
 // One term (a0 F[s] + a1 F[s-1] + a2)(b0 G[s] + b1 G[s+1] + b2) of a product:
 // every product of BuildRHS is one such term and every product of
 // BuildRHSLinear the sum of two.
+// rows are float offsets from the start of the nodal block of shared memory
 struct PTerm {
-  const float *F, *Fm, *Gs, *Gp;
+  int F, Fm, Gs, Gp;
   float a0, a1, a2, b0, b1, b2;
 };
 
-__device__ __forceinline__ void term_set(PTerm& T, const float* F, const float* Fm, float a0, float a1, float a2,
-                                         const float* Gs, const float* Gp, float b0, float b1, float b2) {
+__device__ __forceinline__ void term_set(PTerm& T, int F, int Fm, float a0, float a1, float a2, int Gs, int Gp,
+                                         float b0, float b1, float b2) {
   T.F = F; T.Fm = Fm; T.a0 = a0; T.a1 = a1; T.a2 = a2;
   T.Gs = Gs; T.Gp = Gp; T.b0 = b0; T.b1 = b1; T.b2 = b2;
 }
@@ -169,11 +170,11 @@ __device__ __forceinline__ void term_set(PTerm& T, const float* F, const float* 
 // the terms of product p at slot s (level t); rows of the nodal fields
 // U1,U2,U3,B (`nr`) and of the frozen base (`br`: U1b+U_, U2b, U3b, Bb)
 template <bool LINEAR>
-__device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, int NS, const float* nod,
-                                           const float* bnod, const float* Ub, const float* zc, PTerm& T0,
-                                           PTerm& T1) {
-  auto nr = [&](int f, int ss) { return nod + ((size_t)f * NS + ss) * N1; };
-  auto br = [&](int f, int ss) { return bnod + ((size_t)f * NS + ss) * N1; };
+__device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, int NS, const float* Ub,
+                                           const float* zc, PTerm& T0, PTerm& T1) {
+  // the base rows follow the nodal rows in shared memory (x_layout)
+  auto nr = [&](int f, int ss) { return (f * NS + ss) * N1; };
+  auto br = [&](int f, int ss) { return ((4 + f) * NS + ss) * N1; };
   const bool lo = (t >= 1) && (s >= 1);    // Bar/Tilde rows j >= 1 have a level below
   const int sm = lo ? s - 1 : s;
   const float top = (t <= N3 - 2) ? 1.f : 0.f;   // ReinterpolateDirichlet's last row
@@ -182,7 +183,7 @@ __device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, 
   const float tlo = lof * zc[ZC_TILDE_LO * N3 + t], tdi = lof * zc[ZC_TILDE_DI * N3 + t];
   const float hb = 0.5f * lof;
   const float ub = Ub[t], ubm = lo ? Ub[t - 1] : 0.f;
-  const float* z = nr(0, s);   // any valid row for unused pointers
+  const int z = nr(0, s);   // any valid row for unused terms
   term_set(T1, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
   if (!LINEAR) {
     switch (p) {
@@ -246,8 +247,8 @@ __device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, 
   }
 }
 
-__device__ __forceinline__ float term_eval(const PTerm& T, int x) {
-  return (T.a0 * T.F[x] + T.a1 * T.Fm[x] + T.a2) * (T.b0 * T.Gs[x] + T.b1 * T.Gp[x] + T.b2);
+__device__ __forceinline__ float term_eval(const float* rows, const PTerm& T, int x) {
+  return (T.a0 * rows[T.F + x] + T.a1 * rows[T.Fm + x] + T.a2) * (T.b0 * rows[T.Gs + x] + T.b1 * rows[T.Gp + x] + T.b2);
 }
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
@@ -371,17 +372,17 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
         const int t = j0 - 1 + ss[h];
         live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
       }
-      prod_terms<LINEAR>(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, nod, bnod, Ub, zc,
-                         T[h][0], T[h][1]);
+      prod_terms<LINEAR>(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, Ub, zc, T[h][0],
+                         T[h][1]);
     }
     float2 x[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int n = l + G * e;
-      float v0 = term_eval(T[0][0], n), v1 = term_eval(T[1][0], n);
+      float v0 = term_eval(nod, T[0][0], n), v1 = term_eval(nod, T[1][0], n);
       if (LINEAR) {
-        v0 += term_eval(T[0][1], n);
-        v1 += term_eval(T[1][1], n);
+        v0 += term_eval(nod, T[0][1], n);
+        v1 += term_eval(nod, T[1][1], n);
       }
       x[e] = make_float2(v0, v1);
     }
@@ -590,6 +591,7 @@ __global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
 // shared memory ([N3][32] floats per block). The result equals the sequential
 // sweep up to rounding.
 constexpr int kZW = 8;
+constexpr int kZU2 = 4;   // levels loaded ahead in the chunked z kernels
 
 __device__ __forceinline__ void zscan_up(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
   sA[w * 32 + lane] = A;
@@ -620,7 +622,7 @@ __device__ __forceinline__ void zscan_down(float* sA, float* sB, float* sIn, int
 
 // k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
 // FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
-__global__ void __launch_bounds__(kZW * 32) k_z_cn_chunked(StageArgs a) {
+__global__ void __launch_bounds__(kZW * 32, 3) k_z_cn_chunked(StageArgs a) {
   const Geo g = a.g;
   extern __shared__ float zsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -679,10 +681,10 @@ __global__ void __launch_bounds__(kZW * 32) k_z_cn_chunked(StageArgs a) {
   float bm1 = (f == 2 && js >= 1 && js < N3) ? bc[(js - 1) * S2] : 0.f;
   float w0 = (f == 3 && js < N3) ? wc[js * S2] : 0.f;
   float A = 1.f, B = 0.f;
-  for (int j0 = js; j0 < je; j0 += kZU) {
-    float bu[kZU], br[kZU], bo[kZU], bp[kZU], bx[kZU], bi[kZU];
+  for (int j0 = js; j0 < je; j0 += kZU2) {
+    float bu[kZU2], br[kZU2], bo[kZU2], bp[kZU2], bx[kZU2], bi[kZU2];
 #pragma unroll
-    for (int i = 0; i < kZU; i++) {
+    for (int i = 0; i < kZU2; i++) {
       const int j = j0 + i;
       const bool in = j < je, nx = j + 1 < N3 && in;
       bu[i] = nx ? uc[(j + 1) * S2] : 0.f;
@@ -699,7 +701,7 @@ __global__ void __launch_bounds__(kZW * 32) k_z_cn_chunked(StageArgs a) {
       if (f == 3) bx[i] = nx ? wc[(j + 1) * S2] : 0.f;
     }
 #pragma unroll
-    for (int i = 0; i < kZU; i++) {
+    for (int i = 0; i < kZU2; i++) {
       const int j = j0 + i;
       if (j >= je) break;
       const float up = bu[i];
@@ -768,7 +770,7 @@ __global__ void __launch_bounds__(kZW * 32) k_z_cn_chunked(StageArgs a) {
 // divergence and the Laplacian factors upward, q downward, then u -= grad q
 // and p += pm q. The two components of a mode are adjacent lanes and
 // exchange q; u3_{j+1} at a chunk's top uses the next chunk's q from the scan.
-__global__ void __launch_bounds__(kZW * 32) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
+__global__ void __launch_bounds__(kZW * 32, 3) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
                                                            const float* zc, const float* fa, const float* fc,
                                                            const float* inv_den, const float* kx, const float* ky,
                                                            float pm) {
