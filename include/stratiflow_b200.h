@@ -127,6 +127,14 @@ int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const f
 /* nsteps x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41) */
 int sf_step_linear(sf_solver* s, int nsteps);
 
+/* Tangent-linear batch (no counterpart in the reference, whose
+ * TimeStepLinear keeps its base frozen, IMEXRK.h:334-352): with nbase > 0,
+ * sf_step advances runs 0..nbase-1 by TimeStep and every run r >= nbase by
+ * TimeStepLinear about the live state of run (r - nbase) % nbase at the same
+ * RK stage, i.e. the exact derivative of the discrete step map applied to the
+ * perturbation in run r. nbase must divide nrun; 0 switches it off. */
+int sf_set_tangent(sf_solver* s, int nbase);
+
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 
@@ -159,6 +167,47 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len);
 int sf_remove_divergence_noalloc(const sf_grid* grid, const sf_flow* flow, double pressure_multiplier,
                                  void* u1, void* u2, void* u3, const void* p_in, void* p_out,
                                  void* stream);
+
+/* ---- device state vectors (StateVector algebra, StateVector.h:40-149) ----
+ * A store holds nvec states of one grid on the device, each in the kept
+ * layout [5][N3][plane] (u1,u2,u3,b,p), and shares the stream of the solver
+ * it was created from. Reductions accumulate in FP64. These are the Krylov
+ * bases and iterates of the Newton-Krylov, Arnoldi and continuation drivers,
+ * which in the reference are host std::vector<StateVector> (NewtonKrylov.h:239). */
+typedef struct sf_vecs sf_vecs;
+int sf_vecs_create(sf_solver* like, int nvec, sf_vecs** out);
+int sf_vecs_destroy(sf_vecs* v);
+int sf_vecs_count(sf_vecs* v, int* n);
+/* device address of vector i */
+int sf_vecs_device(sf_vecs* v, int i, void** ptr);
+/* CopyFromSolver / CopyToSolver (StateVector.h:511-543): runs
+ * run..run+count-1 <-> vectors i..i+count-1 */
+int sf_vecs_from_run(sf_vecs* v, int i, sf_solver* s, int run, int count);
+int sf_vecs_to_run(sf_vecs* v, int i, sf_solver* s, int run, int count);
+int sf_vecs_copy(sf_vecs* v, int dst, sf_vecs* w, int src);
+int sf_vecs_set_host(sf_vecs* v, int i, const float* host);
+int sf_vecs_get_host(sf_vecs* v, int i, float* host);
+/* Range operations act on `count` consecutive vectors in one launch.
+ * StateVector::MulAdd (StateVector.h:67-78): v[y+k] += alpha * w[x+k], u1..b */
+int sf_vecs_axpy(sf_vecs* v, int y, double alpha, sf_vecs* w, int x, int count);
+/* v[y+k] = a v[y+k] + b w[x+k] on all five fields */
+int sf_vecs_lincomb(sf_vecs* v, int y, double a, double b, sf_vecs* w, int x, int count);
+/* StateVector::operator*= (StateVector.h:80-91) on all five fields */
+int sf_vecs_scale(sf_vecs* v, int i, double alpha, int count);
+/* out[k] = StateVector::Dot(v[first+k], w[x]) (StateVector.h:122-134), FP64 */
+int sf_vecs_dots(sf_vecs* v, int first, int count, sf_vecs* w, int x, double Ri, double* out);
+/* *out = sum_k StateVector::Dot(v[a+k], w[b+k]), FP64 */
+int sf_vecs_dot_sum(sf_vecs* v, int a, sf_vecs* w, int b, int count, double Ri, double* out);
+/* StateVector::EnforceBCs (StateVector.h:415-421) */
+int sf_vecs_enforce_bcs(sf_vecs* v, int i, int count);
+/* StateVector::RemovePhaseShift (StateVector.h:103-120); computes the shift
+ * from u1(1,0,N3/2) unless use_given, and returns it in *shift */
+int sf_vecs_phase_shift(sf_vecs* v, int i, int use_given, double* shift);
+/* RemoveAverage (Integration.h:236-240) of field 0 (u1) or 3 (b) */
+int sf_vecs_remove_average(sf_vecs* v, int i, int field, double L3);
+/* zero the p field of vectors i..i+count-1 */
+int sf_vecs_zero_pressure(sf_vecs* v, int i, int count);
+int sf_vecs_synchronize(sf_vecs* v);
 
 /* waits for all work queued on the solver's stream */
 int sf_synchronize(sf_solver* s);

@@ -30,6 +30,10 @@ EXPORTS = [
     "sf_set_state_device", "sf_prepare", "sf_remove_divergence", "sf_step", "sf_set_base",
     "sf_step_linear", "sf_energy", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
     "sf_profile_step", "sf_profile_names", "sf_remove_divergence_noalloc",
+    "sf_vecs_create", "sf_vecs_destroy", "sf_vecs_count", "sf_vecs_device", "sf_vecs_from_run", "sf_vecs_to_run",
+    "sf_vecs_copy", "sf_vecs_set_host", "sf_vecs_get_host", "sf_vecs_axpy", "sf_vecs_lincomb", "sf_vecs_scale",
+    "sf_vecs_dots", "sf_vecs_dot_sum", "sf_vecs_enforce_bcs", "sf_vecs_phase_shift", "sf_vecs_remove_average",
+    "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
 ]
 
 
@@ -72,6 +76,14 @@ def load_library(path: str | None = None):
         "sf_stream": [vp, C.POINTER(vp)], "sf_launch_count": [vp, C.POINTER(C.c_longlong)],
         "sf_profile_step": [vp, i, i, i, dp, C.POINTER(i)], "sf_profile_names": [vp, C.c_char_p, C.c_size_t],
         "sf_remove_divergence_noalloc": [C.POINTER(_Grid), C.POINTER(_Flow), d, vp, vp, vp, vp, vp, vp],
+        "sf_vecs_create": [vp, i, C.POINTER(vp)], "sf_vecs_destroy": [vp], "sf_vecs_count": [vp, C.POINTER(i)],
+        "sf_vecs_device": [vp, i, C.POINTER(vp)], "sf_vecs_from_run": [vp, i, vp, i, i], "sf_vecs_to_run": [vp, i, vp, i, i],
+        "sf_vecs_copy": [vp, i, vp, i], "sf_vecs_set_host": [vp, i, fp], "sf_vecs_get_host": [vp, i, fp],
+        "sf_vecs_axpy": [vp, i, d, vp, i, i], "sf_vecs_lincomb": [vp, i, d, d, vp, i, i],
+        "sf_vecs_scale": [vp, i, d, i], "sf_vecs_dots": [vp, i, i, vp, i, d, dp],
+        "sf_vecs_dot_sum": [vp, i, vp, i, i, d, dp], "sf_vecs_enforce_bcs": [vp, i, i],
+        "sf_vecs_phase_shift": [vp, i, i, dp], "sf_vecs_remove_average": [vp, i, i, d], "sf_vecs_synchronize": [vp],
+        "sf_vecs_zero_pressure": [vp, i, i], "sf_set_tangent": [vp, i],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -212,6 +224,10 @@ class IMEXRK:
                 for x in (u1, u2, u3, b)]
         _check(load_library().sf_set_base(self._h, int(run), *[_fptr(x) for x in arrs]))
 
+    def set_tangent(self, nbase):
+        """Runs >= nbase advance linearised about the live run (r - nbase) % nbase."""
+        _check(load_library().sf_set_tangent(self._h, int(nbase)))
+
     def TimeStepLinear(self, n=1):
         """n x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41); asynchronous."""
         _check(load_library().sf_step_linear(self._h, int(n)))
@@ -260,5 +276,80 @@ class IMEXRK:
         return n.value
 
 
-__all__ = ["IMEXRK", "SFError", "load_library", "EXPORTS", "vertical_points",
+class Vecs:
+    """A device store of n states of `solver`'s grid (sf_vecs_*): the
+    StateVector algebra of StateVector.h:40-149, states in the kept layout
+    [5][N3][plane]."""
+
+    def __init__(self, solver: IMEXRK, n: int):
+        self.solver = solver
+        self.n = int(n)
+        self.shape = (5, solver.N3, solver.plane)
+        self._h = C.c_void_p()
+        _check(load_library().sf_vecs_create(solver._h, self.n, C.byref(self._h)))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and h.value:
+            load_library().sf_vecs_destroy(h)
+            self._h = C.c_void_p()
+
+    def set(self, i, a):
+        a = np.ascontiguousarray(a, dtype=np.complex64).reshape(self.shape)
+        _check(load_library().sf_vecs_set_host(self._h, int(i), _fptr(a)))
+
+    def get(self, i):
+        out = np.zeros(self.shape, dtype=np.complex64)
+        _check(load_library().sf_vecs_get_host(self._h, int(i), _fptr(out)))
+        return out
+
+    def from_run(self, i, run, count=1):
+        _check(load_library().sf_vecs_from_run(self._h, int(i), self.solver._h, int(run), int(count)))
+
+    def to_run(self, i, run, count=1):
+        _check(load_library().sf_vecs_to_run(self._h, int(i), self.solver._h, int(run), int(count)))
+
+    def copy(self, dst, other: "Vecs", src):
+        _check(load_library().sf_vecs_copy(self._h, int(dst), other._h, int(src)))
+
+    def axpy(self, y, alpha, other: "Vecs", x, count=1):
+        _check(load_library().sf_vecs_axpy(self._h, int(y), float(alpha), other._h, int(x), int(count)))
+
+    def lincomb(self, y, a, b, other: "Vecs", x, count=1):
+        _check(load_library().sf_vecs_lincomb(self._h, int(y), float(a), float(b), other._h, int(x), int(count)))
+
+    def scale(self, i, alpha, count=1):
+        _check(load_library().sf_vecs_scale(self._h, int(i), float(alpha), int(count)))
+
+    def dots(self, first, count, other: "Vecs", x, Ri):
+        out = np.zeros(int(count))
+        _check(load_library().sf_vecs_dots(self._h, int(first), int(count), other._h, int(x), float(Ri),
+                                           out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def dot_sum(self, a, other: "Vecs", b, count, Ri):
+        out = C.c_double()
+        _check(load_library().sf_vecs_dot_sum(self._h, int(a), other._h, int(b), int(count), float(Ri),
+                                               C.byref(out)))
+        return out.value
+
+    def enforce_bcs(self, i, count=1):
+        _check(load_library().sf_vecs_enforce_bcs(self._h, int(i), int(count)))
+
+    def phase_shift(self, i, shift=None):
+        s = C.c_double(0.0 if shift is None else float(shift))
+        _check(load_library().sf_vecs_phase_shift(self._h, int(i), int(shift is not None), C.byref(s)))
+        return s.value
+
+    def remove_average(self, i, field, L3):
+        _check(load_library().sf_vecs_remove_average(self._h, int(i), int(field), float(L3)))
+
+    def zero_pressure(self, i, count=1):
+        _check(load_library().sf_vecs_zero_pressure(self._h, int(i), int(count)))
+
+    def synchronize(self):
+        _check(load_library().sf_vecs_synchronize(self._h))
+
+
+__all__ = ["IMEXRK", "Vecs", "SFError", "load_library", "EXPORTS", "vertical_points",
            "vertical_points_fractional", "neumann_profile", "background_profile", "kept_modes"]

@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstratiflow_b200.so")
-SOURCES = ["sf_solver.cu", "sf_kernels.cu", "sf_noalloc.cu"]
+SOURCES = ["sf_solver.cu", "sf_kernels.cu", "sf_noalloc.cu", "sf_vecs.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
@@ -32,15 +32,33 @@ def needs_build() -> bool:
     return any(os.path.getmtime(f) > t for f in _inputs())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not needs_build():
-        return LIB
-    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-           "--expt-relaxed-constexpr", "-o", LIB]
-    if verbose:
-        cmd += ["-Xptxas", "-v"]
-    cmd += [os.path.join(CSRC, s) for s in SOURCES]
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libstratiflow_host.so")
+
+
+def build_host(force: bool = False) -> str:
+    """The C++ drivers (host/stratiflow.hpp, host/sf_host.cpp), linked against
+    libstratiflow_b200.so."""
+    srcs = [os.path.join(HOST, f) for f in os.listdir(HOST) if f.endswith((".cpp", ".hpp"))]
+    if (not force and os.path.exists(HOST_LIB)
+            and all(os.path.getmtime(f) <= os.path.getmtime(HOST_LIB) for f in srcs + [LIB])):
+        return HOST_LIB
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I", os.path.join(HERE, "..", "include"),
+           os.path.join(HOST, "sf_host.cpp"), "-L", HERE, "-lstratiflow_b200", "-Wl,-rpath,$ORIGIN",
+           "-o", HOST_LIB]
     subprocess.check_call(cmd)
+    return HOST_LIB
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or needs_build():
+        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+               "--expt-relaxed-constexpr", "-o", LIB]
+        if verbose:
+            cmd += ["-Xptxas", "-v"]
+        cmd += [os.path.join(CSRC, s) for s in SOURCES]
+        subprocess.check_call(cmd)
+    build_host(force)
     return LIB
 
 

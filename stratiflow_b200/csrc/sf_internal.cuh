@@ -68,6 +68,9 @@ struct StageArgs {
   const float* base;    // nrun x 4 x N3 x N2 x N1 (linear step only)
   int stage;
   int linear;
+  int tlm;          // tangent-linear batch: runs < tlm are nonlinear bases, run r >= tlm
+                    // is linearised about the current state of run (r - tlm) % tlm
+  int run_offset;   // first run of this launch (x pass)
   float h, hz, hb, cv, cb, pm;
 };
 

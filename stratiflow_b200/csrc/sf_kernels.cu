@@ -136,14 +136,17 @@ struct XLayout {  // shared-memory carve-up of k_xpass
   size_t hat_off, buf_off, nod_off, base_off, bytes;
 };
 
-__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int ngroups) {
+__host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int ngroups,
+                                            int tlm = 0) {
   XLayout L;
   L.nprod = dim3 ? P_COUNT : 6;
   L.nrows = prod_rows(L.nprod, S);
   size_t off = 0;
   // transformed products, one row of K1 per (product, slot); before phase B
-  // the same bytes stage the input rows of phase A (4 x (S+2) x K1)
-  size_t hat = sizeof(float2) * (size_t)L.nrows * K1, stage = sizeof(float2) * (size_t)4 * (S + 2) * K1;
+  // the same bytes stage the input rows of phase A (4 x (S+2) x K1, twice
+  // that when the base rows of a tangent-linear batch come along)
+  size_t hat = sizeof(float2) * (size_t)L.nrows * K1,
+         stage = sizeof(float2) * (size_t)(tlm ? 8 : 4) * (S + 2) * K1;
   L.hat_off = off;  off += (hat > stage ? hat : stage);
   L.buf_off = off;  off += sizeof(float2) * (size_t)ngroups * bufstride;
   L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
@@ -266,36 +269,39 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   const int NGB = blockDim.x / G;   // lane groups per block
   const Geo g = a.g;
   extern __shared__ __align__(16) unsigned char xsm[];
-  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB);
+  const int tlm = LINEAR ? a.tlm : 0;   // base rows from a live run of this batch
+  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB, tlm);
   float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
-  float2* stg = hat;                                           // phase A input rows [4][S+2][K1]
+  float2* stg = hat;                                           // phase A input rows [4 or 8][S+2][K1]
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
   const int K1 = g.K1, N3 = g.N3;
   const int j0 = blockIdx.x * S;
   const int y = blockIdx.y;
-  const int run = blockIdx.z;
+  const int run = blockIdx.z + a.run_offset;
+  const int brun = tlm ? (run - tlm) % tlm : run;   // run that holds the base state
   const int gid = threadIdx.x / G, l = threadIdx.x % G;
   float2* buf = reinterpret_cast<float2*>(xsm + L.buf_off) + (size_t)gid * BUF;
   const float* Ub = a.Ubar + (size_t)run * N3;
   const float* zc = a.zc;
   const int NS = S + 2;
-  const int nf = g.dim3 ? 4 : 4;
+  const int nf = tlm ? 8 : 4;   // own u1,u2,u3,b (and the base run's)
 
   // ---- stage the input rows (u1,u2,u3,b at levels j0-1 .. j0+S) ----
   for (int i = threadIdx.x; i < nf * NS * K1; i += blockDim.x) {
-    const int f = i / (NS * K1), r = i - f * NS * K1, s = r / K1, k = r - s * K1;
+    const int fb = i / (NS * K1), r = i - fb * NS * K1, s = r / K1, k = r - s * K1;
+    const int f = fb & 3, rr = fb < 4 ? run : brun;
     const int t = j0 - 1 + s;
     float2* d = stg + i;
     if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
       *d = make_float2(0.f, 0.f);
     } else if (g.dim3) {
-      cp_async8(d, a.mixin + (((size_t)(run * 4 + f) * N3 + t) * g.N2 + y) * K1 + k);
+      cp_async8(d, a.mixin + (((size_t)(rr * 4 + f) * N3 + t) * g.N2 + y) * K1 + k);
     } else {
-      cp_async8(d, a.S + ((size_t)(run * 5 + f) * N3 + t) * g.Pp + k);
+      cp_async8(d, a.S + ((size_t)(rr * 5 + f) * N3 + t) * g.Pp + k);
     }
   }
-  if (LINEAR) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
+  if (LINEAR && !tlm) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
     for (int i = threadIdx.x; i < 4 * NS * N1; i += blockDim.x) {
       int f = i / (NS * N1), r = i - f * NS * N1, s = r / N1, x = r - s * N1;
       int t = j0 - 1 + s;
@@ -311,15 +317,17 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   __syncthreads();
 
   // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
-  const int ntA = NS * 2;
+  // (and of the base run's fields for a tangent-linear batch)
+  const int ntA = NS * (tlm ? 4 : 2);
   for (int base = 0; base < ntA; base += NGB) {
     const int task = base + gid;
     const bool valid = task < ntA;
-    const int s = valid ? task >> 1 : 0, pr = task & 1;
+    const int s = valid ? task % NS : 0, pr4 = valid ? task / NS : 0;
+    const int pr = pr4 & 1, ofs = (pr4 >> 1) * 4;   // ofs 4: base rows
     const int fA = pr == 0 ? 0 : 3;       // u1 | b
     const int fB = pr == 0 ? 2 : 1;       // u3 | u2
-    const float2* srcA = stg + ((size_t)fA * NS + s) * K1;
-    const float2* srcB = stg + ((size_t)fB * NS + s) * K1;
+    const float2* srcA = stg + ((size_t)(ofs + fA) * NS + s) * K1;
+    const float2* srcB = stg + ((size_t)(ofs + fB) * NS + s) * K1;
     float2 x[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
@@ -338,12 +346,16 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
     }
     reg_fft<N1, true>(x, buf, a.tw, l);
     if (valid) {
-      float* rA = nod + ((size_t)fA * NS + s) * N1;
-      float* rB = nod + ((size_t)fB * NS + s) * N1;
+      float* rows = ofs ? bnod : nod;
+      float* rA = rows + ((size_t)fA * NS + s) * N1;
+      float* rB = rows + ((size_t)fB * NS + s) * N1;
+      const int t = j0 - 1 + s;
+      // the base's U1 row carries U_ (nnTemp = U1_tot + U_, IMEXRK.cpp:212)
+      const float add = (ofs && fA == 0 && t >= 0 && t < N3) ? a.Ubar[(size_t)brun * N3 + t] : 0.f;
 #pragma unroll
       for (int sl = 0; sl < E; sl++) {
         const int xo = reg_fft_out_index<N1>(l, sl);
-        rA[xo] = x[sl].x;
+        rA[xo] = x[sl].x + add;
         rB[xo] = x[sl].y;
       }
     }
@@ -1111,8 +1123,9 @@ __global__ void k_inner(Geo g, const float2* __restrict__ Sa, const float2* __re
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
 template <int N1, bool LIN>
-static void xpass_launch(const StageArgs& a, cudaStream_t st) {
+static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
   const Geo& g = a.g;
+  const int tlm = LIN ? a.tlm : 0;
   constexpr int G = FFTShape<N1>::G, BUF = fft_buf_stride<N1>();
   const int nprod = g.dim3 ? P_COUNT : 6;
   // threads: enough lane groups for all phase-A transforms of a slab (one
@@ -1122,7 +1135,7 @@ static void xpass_launch(const StageArgs& a, cudaStream_t st) {
     int t = ((groups * G + 31) / 32) * 32;
     return t < 64 ? 64 : (t > kXMaxThreads ? kXMaxThreads : t);
   };
-  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, threads(S) / G).bytes; };
+  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, threads(S) / G, tlm).bytes; };
   (void)nprod;
   // largest slab whose shared memory lets two blocks share an SM, then
   // smaller slabs while the grid would leave SMs idle
@@ -1133,23 +1146,38 @@ static void xpass_launch(const StageArgs& a, cudaStream_t st) {
   if (g.dim3 && S > 4) S = 4;
   for (int i = 0; i < 5; i++) {
     if (cand[i] >= S) continue;
-    if ((long long)((g.N3 + S - 1) / S) * g.N2 * g.nrun >= 2 * 148) break;
+    if ((long long)((g.N3 + S - 1) / S) * g.N2 * nruns >= 2 * 148) break;
     S = cand[i];
   }
-  dim3 grid(cdiv(g.N3, S), g.N2, g.nrun);
+  dim3 grid(cdiv(g.N3, S), g.N2, nruns);
   k_xpass<N1, LIN><<<grid, threads(S), bytes(S), st>>>(a, S);
 }
 
-static int launch_xpass(const StageArgs& a, cudaStream_t st) {
-  const bool L = a.linear != 0;
+static void launch_xpass_runs(const StageArgs& a, bool L, int nruns, cudaStream_t st) {
   switch (a.g.N1) {
-    case 16: L ? xpass_launch<16, true>(a, st) : xpass_launch<16, false>(a, st); break;
-    case 32: L ? xpass_launch<32, true>(a, st) : xpass_launch<32, false>(a, st); break;
-    case 64: L ? xpass_launch<64, true>(a, st) : xpass_launch<64, false>(a, st); break;
-    case 128: L ? xpass_launch<128, true>(a, st) : xpass_launch<128, false>(a, st); break;
-    case 256: L ? xpass_launch<256, true>(a, st) : xpass_launch<256, false>(a, st); break;
-    case 512: L ? xpass_launch<512, true>(a, st) : xpass_launch<512, false>(a, st); break;
+    case 16: L ? xpass_launch<16, true>(a, nruns, st) : xpass_launch<16, false>(a, nruns, st); break;
+    case 32: L ? xpass_launch<32, true>(a, nruns, st) : xpass_launch<32, false>(a, nruns, st); break;
+    case 64: L ? xpass_launch<64, true>(a, nruns, st) : xpass_launch<64, false>(a, nruns, st); break;
+    case 128: L ? xpass_launch<128, true>(a, nruns, st) : xpass_launch<128, false>(a, nruns, st); break;
+    case 256: L ? xpass_launch<256, true>(a, nruns, st) : xpass_launch<256, false>(a, nruns, st); break;
+    case 512: L ? xpass_launch<512, true>(a, nruns, st) : xpass_launch<512, false>(a, nruns, st); break;
   }
+}
+
+// the x pass of every run: one launch, or for a tangent-linear batch one
+// nonlinear launch for the base runs and one linear launch for the rest
+static int launch_xpass(const StageArgs& a, cudaStream_t st) {
+  if (a.tlm > 0) {
+    StageArgs b = a;
+    b.run_offset = 0;
+    launch_xpass_runs(b, false, a.tlm, st);
+    b.run_offset = a.tlm;
+    launch_xpass_runs(b, true, a.g.nrun - a.tlm, st);
+    return 2;
+  }
+  StageArgs b = a;
+  b.run_offset = 0;
+  launch_xpass_runs(b, a.linear != 0, a.g.nrun, st);
   return 1;
 }
 
@@ -1222,7 +1250,7 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     launch_ifft_y(a, g.nrun, st);
     mark();
   }
-  launch_xpass(a, st);
+  n += launch_xpass(a, st) - 1;   // counts the kernels, the mark below adds one
   mark();
   if (g.dim3) {
     launch_fft_y(a, st);

@@ -49,6 +49,7 @@ struct sf_solver {
   std::vector<double> zN, zfN;   // grid (for inspection)
   int cur = 0;                   // index of the current state buffer
   bool base_set = false;
+  int tlm = 0;                   // tangent-linear batch (sf_set_tangent)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -168,6 +169,8 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.base = s->base;
   a.stage = k;
   a.linear = linear ? 1 : 0;
+  a.tlm = linear ? 0 : s->tlm;
+  a.run_offset = 0;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -203,6 +206,13 @@ static int ensure_graph(sf_solver* s, bool linear, int par) {
   s->launches_per_step[linear] = n;
   return SF_OK;
 }
+
+// accessors for the other translation units (vector store)
+const Geo& sf_solver_geo(const sf_solver* s) { return s->g; }
+const float* sf_solver_zc(const sf_solver* s) { return s->zc; }
+float2* sf_solver_state(sf_solver* s, int run) { return s->S[s->cur] + (size_t)run * 5 * s->g.fblk; }
+cudaStream_t sf_solver_stream(const sf_solver* s) { return s->st; }
+const std::vector<double>& sf_solver_z(const sf_solver* s, int which) { return which == 0 ? s->zN : s->zfN; }
 
 extern "C" {
 
@@ -606,6 +616,17 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);
+  return SF_OK;
+}
+
+int sf_set_tangent(sf_solver* s, int nbase) {
+  if (!s) return fail(SF_EINVAL, "null solver");
+  if (nbase < 0 || (nbase > 0 && (s->g.nrun <= nbase || s->g.nrun % nbase != 0)))
+    return fail(SF_EINVAL, "nbase must divide nrun and be smaller than it (0 switches the mode off)");
+  if (nbase != s->tlm) {
+    s->tlm = nbase;
+    drop_graphs(s);
+  }
   return SF_OK;
 }
 

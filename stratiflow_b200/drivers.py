@@ -1,0 +1,244 @@
+"""Newton-Krylov, periodic-orbit and pseudo-arclength drivers (the C++
+library libstratiflow_host.so, built from host/) and the continuation loop.
+
+States are numpy complex64 arrays in the kept layout [5][N3][plane] (one
+state) or [M][5][N3][plane] (M shooting segments).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import time
+
+import numpy as np
+
+from . import SFError, load_library
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+HOST_LIB = os.path.join(HERE, "libstratiflow_host.so")
+_host = None
+
+
+def load_host():
+    global _host
+    if _host is None:
+        load_library()   # the CUDA library first (and its error if missing)
+        if not os.path.exists(HOST_LIB):
+            raise SFError(f"{HOST_LIB} is missing: build it with `python -m stratiflow_b200.build`")
+        L = C.CDLL(HOST_LIB)
+        dp, fp, i, d = C.POINTER(C.c_double), C.c_void_p, C.c_int, C.c_double
+        L.sfh_last_error.restype = C.c_char_p
+        L.sfh_newton_fixed.argtypes = [dp, i, d, i, fp, dp, fp, dp, i]
+        L.sfh_periodic_orbit.argtypes = [dp, i, d, fp, dp, fp, dp, dp, i]
+        L.sfh_arclength.argtypes = [dp, i, d, fp, d, fp, d, d, fp, d, dp, fp, dp, dp, i]
+        L.sfh_evolve.argtypes = [dp, i, d, d, fp, fp]
+        L.sfh_evolve_tangent.argtypes = [dp, i, d, d, fp, fp, fp]
+        for f in ("sfh_newton_fixed", "sfh_periodic_orbit", "sfh_arclength", "sfh_evolve", "sfh_evolve_tangent"):
+            getattr(L, f).restype = C.c_int
+        _host = L
+    return _host
+
+
+BACKGROUNDS = {"tanh": 0, "holmboe": 1, "linear": 2}
+
+
+class Flow:
+    """Grid + flow parameters of a driver call (Parameters.h:6-43)."""
+
+    def __init__(self, N1, N2, N3, L1, L2, L3, Re, Pr, Ri, dt, background="tanh"):
+        self.N1, self.N2, self.N3 = int(N1), int(N2), int(N3)
+        self.L1, self.L2, self.L3 = float(L1), float(L2), float(L3)
+        self.Re, self.Pr, self.Ri, self.dt = float(Re), float(Pr), float(Ri), float(dt)
+        self.background = background
+        K1 = self.N1 // 3
+        K2 = 2 * (self.N2 // 3) - 1 if self.N2 > 1 else 1
+        self.plane = (K1 * K2 + 15) // 16 * 16
+        self.state_shape = (5, self.N3, self.plane)
+
+    def array(self):
+        return np.array([self.N1, self.N2, self.N3, self.L1, self.L2, self.L3, self.Re, self.Pr, self.Ri,
+                         self.dt, BACKGROUNDS[self.background]], dtype=np.float64)
+
+
+class NKOptions:
+    """jacobian: "tangent" (exact actions by the tangent-linear batch) or
+    "fd" (finite differences with step fd_eps |x|, NewtonKrylov.h:218-235)."""
+
+    def __init__(self, max_newton=20, krylov=80, target=1e-6, gmres_tol=0.01, Delta=100.0, fd_eps=3e-4,
+                 jacobian="tangent"):
+        assert jacobian in ("tangent", "fd")
+        self.v = np.array([max_newton, krylov, target, gmres_tol, Delta, fd_eps, 0.0 if jacobian == "tangent" else 1.0],
+                          dtype=np.float64)
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _segments(flow, x, M):
+    x = np.ascontiguousarray(x, dtype=np.complex64)
+    if x.shape == flow.state_shape:
+        x = np.broadcast_to(x, (M,) + flow.state_shape).copy()
+    assert x.shape == (M,) + flow.state_shape, x.shape
+    return x
+
+
+def _stats(st):
+    n = int(st[7])
+    return {"newton_iterations": int(st[0]), "jacobian_actions": int(st[1]), "integrations": int(st[2]),
+            "seconds": float(st[3]), "integration_seconds": float(st[4]), "residual": float(st[5]),
+            "converged": bool(st[6] > 0.5), "residuals": [float(v) for v in st[8:8 + n]]}
+
+
+def _call(rc):
+    if rc != 0:
+        raise SFError(load_host().sfh_last_error().decode(errors="replace"))
+
+
+def newton_fixed(flow: Flow, x, T, M=1, opts: NKOptions | None = None, constrain=True):
+    """Phi_T(x) = x by Newton-Krylov with M shooting segments
+    (BasicNewtonKrylov, BasicNewtonKrylov.h:5-14; constraints of
+    PseudoArclength.h:15-20)."""
+    L = load_host()
+    xs = _segments(flow, x, M)
+    out = np.zeros_like(xs)
+    st = np.zeros(8 + 64)
+    opts = opts or NKOptions()
+    _call(L.sfh_newton_fixed(_dp(flow.array()), M, float(T), int(constrain), _fp(xs), _dp(opts.v), _fp(out),
+                             _dp(st), len(st)))
+    return out, _stats(st)
+
+
+def periodic_orbit(flow: Flow, x, T0, M=16, opts: NKOptions | None = None):
+    """FindPeriodic (FindPeriodic.cpp:4-28) by multiple shooting: returns the
+    M segments, the period and the statistics."""
+    L = load_host()
+    xs = _segments(flow, x, M)
+    out = np.zeros_like(xs)
+    T = C.c_double()
+    st = np.zeros(8 + 64)
+    opts = opts or NKOptions()
+    _call(L.sfh_periodic_orbit(_dp(flow.array()), M, float(T0), _fp(xs), _dp(opts.v), _fp(out), C.byref(T),
+                               _dp(st), len(st)))
+    return out, T.value, _stats(st)
+
+
+def arclength_correct(flow: Flow, x0, Ri0, v, vRi, ds, guess, Ri_guess, T, M=1, opts: NKOptions | None = None):
+    """One corrector of the pseudo-arclength continuation
+    (PseudoArclength.h:6-42)."""
+    L = load_host()
+    X0, V, G = (_segments(flow, a, M) for a in (x0, v, guess))
+    out = np.zeros_like(G)
+    ri = C.c_double()
+    st = np.zeros(8 + 64)
+    opts = opts or NKOptions()
+    _call(L.sfh_arclength(_dp(flow.array()), M, float(T), _fp(X0), float(Ri0), _fp(V), float(vRi), float(ds),
+                          _fp(G), float(Ri_guess), _dp(opts.v), _fp(out), C.byref(ri), _dp(st), len(st)))
+    return out, ri.value, _stats(st)
+
+
+def evolve(flow: Flow, x, tau, Ri=None, M=1):
+    L = load_host()
+    xs = _segments(flow, x, M)
+    out = np.zeros_like(xs)
+    _call(L.sfh_evolve(_dp(flow.array()), M, float(tau), float(flow.Ri if Ri is None else Ri), _fp(xs),
+                       _fp(out)))
+    return out
+
+
+def evolve_tangent(flow: Flow, x, dx, tau, Ri=None, M=1):
+    """Phi'(x) dx over tau for each of the M segments (exact tangent-linear
+    integration about the moving base)."""
+    L = load_host()
+    xs, ds = _segments(flow, x, M), _segments(flow, dx, M)
+    out = np.zeros_like(xs)
+    _call(L.sfh_evolve_tangent(_dp(flow.array()), M, float(tau), float(flow.Ri if Ri is None else Ri), _fp(xs),
+                               _fp(ds), _fp(out)))
+    return out
+
+
+# ------------------------------------------------------------ continuation
+def ext_dot(flow: Flow, a, b, Ri):
+    """ExtendedStateVector::Dot (ExtendedStateVector.h:12-15) on host arrays:
+    StateVector::Dot (StateVector.h:122-134) of the states plus p p'."""
+    from .grid import vertical_points, vertical_points_fractional
+    xa, pa = a
+    xb, pb = b
+    N3 = flow.N3
+    z = vertical_points(flow.L3, N3)
+    zf = vertical_points_fractional(flow.L3, N3)
+    wzn = np.zeros(N3)
+    wzn[1:N3 - 1] = z[2:N3] - z[1:N3 - 1]
+    wzd = np.zeros(N3)
+    wzd[2:N3 - 1] = zf[2:N3 - 1] - zf[1:N3 - 2]
+    K1 = flow.N1 // 3
+    K2 = 2 * (flow.N2 // 3) - 1 if flow.N2 > 1 else 1
+    P = K1 * K2
+    wm = np.zeros(flow.plane)
+    wm[:P] = 2.0
+    wm[0] = 1.0
+    xa = xa.reshape((-1,) + flow.state_shape)
+    xb = xb.reshape((-1,) + flow.state_shape)
+    tot = 0.0
+    for f, (wz, wf) in enumerate(((wzn, 1.0), (wzn, 1.0), (wzd, 1.0), (wzn, Ri))):
+        if f == 1 and flow.N2 == 1:
+            continue
+        t = (xa[:, f].real.astype(np.float64) * xb[:, f].real + xa[:, f].imag.astype(np.float64) * xb[:, f].imag)
+        tot += wf * float(np.einsum("sjm,j,m->", t, wz, wm))
+    return tot + pa * pb
+
+
+def secant_predictor(flow: Flow, p1, p2, ds):
+    """PseudoArclength.cpp:33-61: unit tangent from two converged points in
+    the extended norm; guess = x2 + ds v. Returns (guess, tangent)."""
+    (x1, r1), (x2, r2) = p1, p2
+    dx = x2.astype(np.complex128) - x1
+    if r2 == r1:
+        n = np.sqrt(ext_dot(flow, (dx, 0.0), (dx, 0.0), r2))
+        v = (dx / n, 0.0)
+    else:
+        vx = dx / (r2 - r1)
+        vp = 1.0 / np.sqrt(1.0 + ext_dot(flow, (vx, 0.0), (vx, 0.0), r2))
+        vx = vx * vp
+        if r2 < r1:
+            vx, vp = -vx, -vp
+        v = (vx, vp)
+    guess = (x2 + ds * v[0], r2 + ds * v[1])
+    return (guess[0].astype(np.complex64), guess[1]), (v[0].astype(np.complex64), v[1])
+
+
+def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, predictor=None, log=None):
+    """Pseudo-arclength continuation from two converged points
+    ((x, Ri), (x, Ri)). `predictor(history, ds)` may replace the secant: it
+    gets the converged points so far and returns a guess (x, Ri); the secant
+    tangent is always used for the arclength constraint. Returns the points
+    and the per-point statistics."""
+    pts = list(start_points)
+    stats = []
+    for k in range(npoints):
+        t0 = time.perf_counter()
+        sec_guess, (vx, vp) = secant_predictor(flow, pts[-2], pts[-1], ds)
+        guess = predictor(pts, ds) if predictor is not None else sec_guess
+        used = "learned" if predictor is not None else "secant"
+        x, Ri, st = arclength_correct(flow, pts[-1][0], pts[-1][1], vx, vp, ds, guess[0], guess[1], T, M, opts)
+        if not st["converged"] and predictor is not None:
+            # the secant predictor remains the fallback
+            x, Ri, st2 = arclength_correct(flow, pts[-1][0], pts[-1][1], vx, vp, ds, sec_guess[0], sec_guess[1],
+                                           T, M, opts)
+            st2["fallback_from"] = st
+            st = st2
+            used = "secant (fallback)"
+        st["predictor"] = used
+        st["wall_seconds"] = time.perf_counter() - t0
+        st["Ri"] = Ri
+        stats.append(st)
+        pts.append((x.reshape(flow.state_shape) if M == 1 else x, Ri))
+        if log:
+            log(k, st)
+        if not st["converged"]:
+            break
+    return pts, stats

@@ -1,0 +1,216 @@
+// C entry points of the host-side drivers (stratiflow.hpp), used by the
+// Python front end and the benchmarks:
+//   sfh_newton_fixed     BasicNewtonKrylov (BasicNewtonKrylov.h): Phi_T(x) = x
+//   sfh_periodic_orbit   FindPeriodic (FindPeriodic.cpp): Phi_T(x) = x, T unknown
+//   sfh_arclength        one corrector of PseudoArclength (PseudoArclength.cpp:63-68)
+// States cross this interface in the kept layout of include/stratiflow_b200.h,
+// M consecutive states (the shooting segments).
+#include <cstring>
+#include <exception>
+#include <string>
+
+#include "stratiflow.hpp"
+
+using namespace stratiflow;
+
+namespace {
+
+thread_local std::string g_host_err;
+
+Params params_from(const double* a) {
+  Params p;
+  p.N1 = (int)a[0]; p.N2 = (int)a[1]; p.N3 = (int)a[2];
+  p.L1 = a[3]; p.L2 = a[4]; p.L3 = a[5]; p.Re = a[6]; p.Pr = a[7]; p.Ri = a[8]; p.dt = a[9];
+  p.background = (int)a[10];
+  return p;
+}
+
+NKOptions options_from(const double* o) {
+  NKOptions n;
+  if (!o) return n;
+  n.max_newton = (int)o[0];
+  n.krylov = (int)o[1];
+  n.target = o[2];
+  n.gmres_tol = o[3];
+  n.Delta = o[4];
+  n.fd_eps = o[5];
+  n.tangent = o[6] == 0.0;   // 0: tangent-linear Jacobian actions, 1: finite differences
+  return n;
+}
+
+size_t kept_elems(const Params& p) {
+  const int K1 = p.N1 / 3, K2 = p.N2 > 1 ? 2 * (p.N2 / 3) - 1 : 1;
+  const int plane = (K1 * K2 + 15) / 16 * 16;
+  return (size_t)5 * p.N3 * plane;   // complex values of one state
+}
+
+void load(Vec& x, const float* host, const Params& p) {
+  for (int i = 0; i < x.M(); i++) x.set_segment_host(i, host + 2 * kept_elems(p) * i);
+}
+void store(const Vec& x, float* host, const Params& p) {
+  for (int i = 0; i < x.M(); i++) x.get_segment_host(i, host + 2 * kept_elems(p) * i);
+}
+
+// stats layout: [0] newton iterations, [1] Jacobian actions, [2] batched
+// integrations, [3] seconds, [4] seconds inside integrations, [5] final
+// relative residual, [6] converged, [7] number of residuals n, [8..8+n) residuals
+void write_stats(const NKStats& s, double* out, int cap) {
+  if (!out || cap < 8) return;
+  out[0] = s.newton_iterations;
+  out[1] = s.krylov_vectors;
+  out[2] = (double)s.evolutions;
+  out[3] = s.seconds;
+  out[4] = s.evolve_seconds;
+  out[5] = s.residual;
+  out[6] = s.converged ? 1.0 : 0.0;
+  const int n = std::min((int)s.residuals.size(), cap - 8);
+  out[7] = n;
+  for (int i = 0; i < n; i++) out[8 + i] = s.residuals[i];
+}
+
+// BasicNewtonKrylov with the constraints of PseudoArclength (phase, averages)
+class FixedPoint : public NewtonKrylov {
+ public:
+  FixedPoint(const NKOptions& o, double T, bool constrain) : NewtonKrylov(o), T_(T), constrain_(constrain) {}
+  Vec EvalFunction(const Vec& at) override {
+    Vec phi(at);
+    Evolve(at, T_ / at.M(), at.ctx().p.Ri, phi);
+    Vec r = ShootingResidual(phi, at);
+    r.p = 0;
+    return r;
+  }
+  void EnforceConstraints(Vec& at) override {
+    if (!constrain_) return;
+    at.RemovePhaseShift();
+    at.RemoveAverage(0);
+    at.RemoveAverage(3);
+  }
+  // Phi' d_i - d_{i+1}
+  Vec EvalDerivative(const Vec& dir) override {
+    if (!opt.tangent) return NewtonKrylov::EvalDerivative(dir);
+    Vec phi(dir);
+    EvolveTangent(*x0_, dir, T_ / dir.M(), dir.ctx().p.Ri, phi);
+    Vec r = ShootingResidual(phi, dir);
+    r.p = 0;
+    return r;
+  }
+
+ private:
+  double T_;
+  bool constrain_;
+};
+
+}  // namespace
+
+extern "C" {
+
+const char* sfh_last_error(void) { return g_host_err.c_str(); }
+
+// params: N1,N2,N3,L1,L2,L3,Re,Pr,Ri,dt,background; opts: max_newton, krylov,
+// target, gmres_tol, Delta, fd_eps, jacobian (0 tangent-linear, 1 finite differences)
+int sfh_newton_fixed(const double* params, int M, double T, int constrain, const float* guess, const double* opts,
+                     float* out, double* stats, int stats_cap) {
+  try {
+    Params p = params_from(params);
+    Context c(p, M);
+    Vec x(c);
+    load(x, guess, p);
+    x.EnforceBCs();
+    FixedPoint nk(options_from(opts), T, constrain != 0);
+    if (constrain) nk.EnforceConstraints(x);
+    NKStats s = nk.Run(x);
+    store(x, out, p);
+    write_stats(s, stats, stats_cap);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+int sfh_periodic_orbit(const double* params, int M, double T0, const float* guess, const double* opts, float* out,
+                       double* T_out, double* stats, int stats_cap) {
+  try {
+    Params p = params_from(params);
+    Context c(p, M);
+    Vec x(c);
+    load(x, guess, p);
+    x.EnforceBCs();
+    x.p = T0;
+    PeriodicOrbit nk(options_from(opts), x);
+    NKStats s = nk.Run(x);
+    store(x, out, p);
+    if (T_out) *T_out = x.p;
+    write_stats(s, stats, stats_cap);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// One pseudo-arclength corrector: x0 (M states, Ri0) is the last converged
+// point, v (M states, v_Ri) the unit tangent in the extended norm, ds the
+// step, guess (M states, Ri_guess) the predictor. Writes the converged point.
+int sfh_arclength(const double* params, int M, double T, const float* x0, double Ri0, const float* v, double vRi,
+                  double ds, const float* guess, double Ri_guess, const double* opts, float* out, double* Ri_out,
+                  double* stats, int stats_cap) {
+  try {
+    Params p = params_from(params);
+    Context c(p, M);
+    Vec X0(c), V(c), X(c);
+    load(X0, x0, p);
+    X0.p = Ri0;
+    load(V, v, p);
+    V.p = vRi;
+    load(X, guess, p);
+    X.p = Ri_guess;
+    X.EnforceBCs();
+    PseudoArclength nk(options_from(opts), X0, V, ds, T);
+    nk.EnforceConstraints(X);
+    NKStats s = nk.Run(X);
+    store(X, out, p);
+    if (Ri_out) *Ri_out = X.p;
+    write_stats(s, stats, stats_cap);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// The tangent-linear action Phi'(x) dx of the M segments over tau each
+int sfh_evolve_tangent(const double* params, int M, double tau, double Ri, const float* x, const float* dx,
+                       float* out) {
+  try {
+    Params p = params_from(params);
+    Context c(p, M);
+    Vec a(c), d(c), y(c);
+    load(a, x, p);
+    load(d, dx, p);
+    EvolveTangent(a, d, tau, Ri, y);
+    store(y, out, p);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// Evolve M segments over T/M each (for the callers' own experiments)
+int sfh_evolve(const double* params, int M, double tau, double Ri, const float* in, float* out) {
+  try {
+    Params p = params_from(params);
+    Context c(p, M);
+    Vec x(c), y(c);
+    load(x, in, p);
+    Evolve(x, tau, Ri, y);
+    store(y, out, p);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,651 @@
+// C++ front end of stratiflow_b200 over its C-ABI: the reference's solver
+// and driver classes (IMEXRK, StateVector/ExtendedStateVector, NewtonKrylov,
+// PseudoArclengthContinuation, FindPeriodic) with their device state on the
+// GPU and FP64 Krylov numerics on the host.
+//
+// A state here is a multiple-shooting vector: M segments x_0..x_{M-1} of
+// one trajectory (M = 1 is the reference's StateVector) plus one scalar
+// parameter p (the reference's ExtendedStateVector::p: Ri in continuation, the
+// period T in the periodic-orbit search). Every evaluation of the evolution
+// map advances all M segments as the M runs of one batched solver, so one
+// Jacobian action of GMRES costs one batched integration over T/M.
+#pragma once
+
+#include <chrono>
+#include <cmath>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "stratiflow_b200.h"
+
+namespace stratiflow {
+
+inline void check(int rc) {
+  if (rc != SF_OK) throw std::runtime_error(std::string("stratiflow_b200: ") + sf_last_error());
+}
+
+// gridParams + flowParams (Parameters.h:6-43) and the background of the run
+struct Params {
+  int N1 = 256, N2 = 1, N3 = 256;
+  double L1 = 2 * 3.141592653589793 / 0.44, L2 = 3.141592653589793 / 0.44, L3 = 10.0;
+  double Re = 1000, Pr = 1, Ri = 0.12, dt = 0.01;
+  int background = 0;   // 0: B = tanh z, 1: B = tanh 3z, 2: B = z (the reference)
+};
+
+// Field.cpp:21-31 in FP64
+inline std::vector<double> vertical_points_fractional(double L, int N) {
+  std::vector<double> z(N, 0.0), zf(N, 0.0);
+  const double step = 2.0 / (N - 2);
+  for (int i = 0; i < N - 1; i++) {
+    double x = (i == N - 2) ? 1.0 : -1.0 + i * step;
+    z[i + 1] = L * (2.0 * std::pow(x, 7) + x) / 3.0;
+  }
+  double off = (z[1] + z[2]) / 2;
+  for (int i = 1; i < N; i++) z[i] *= -L / off;
+  for (int i = 1; i <= N - 2; i++) zf[i] = 0.5 * (z[i] + z[i + 1]);
+  zf[0] = 2 * zf[1] - zf[2];
+  zf[N - 1] = 2 * zf[N - 2] - zf[N - 3];
+  return zf;
+}
+
+// U_ = tanh z set as Nodal1D::SetValue does (Field.h:661-682), and dB/dz
+inline void background_profiles(const Params& p, std::vector<double>& U, std::vector<double>& dB) {
+  const int N = p.N3;
+  auto zf = vertical_points_fractional(p.L3, N);
+  U.resize(N);
+  dB.resize(N);
+  for (int j = 0; j < N; j++) {
+    U[j] = std::tanh(zf[j]);
+    double c1 = std::cosh(zf[j]), c3 = std::cosh(3 * zf[j]);
+    dB[j] = p.background == 0 ? 1.0 / (c1 * c1) : (p.background == 1 ? 3.0 / (c3 * c3) : 1.0);
+  }
+  U[1] = U[2]; U[0] = U[1]; U[N - 2] = U[N - 3]; U[N - 1] = U[N - 2];
+}
+
+// IMEXRK (IMEXRK.h:31-670) for a batch of runs
+class Solver {
+ public:
+  Solver(const Params& p, int nrun) : p_(p), nrun_(nrun), ri_(nrun, -1.0), dt_(p.dt) {
+    sf_grid g{p.N1, p.N2, p.N3, nrun};
+    sf_flow f{p.L1, p.L2, p.L3, p.Re, p.Pr};
+    check(sf_create(&g, &f, p.dt, 0, &h_));
+    std::vector<double> U, dB;
+    background_profiles(p, U, dB);
+    for (int r = 0; r < nrun; r++) {
+      check(sf_set_background(h_, r, U.data(), dB.data()));
+      set_ri(r, p.Ri);
+    }
+  }
+  ~Solver() { sf_destroy(h_); }
+  Solver(const Solver&) = delete;
+  Solver& operator=(const Solver&) = delete;
+  void set_dt(double dt) {
+    if (std::fabs(dt - dt_) > 1e-14 * dt) {
+      check(sf_set_dt(h_, dt));
+      dt_ = dt;
+    }
+  }
+  void set_ri(int run, double ri) {
+    if (ri != ri_[run]) {
+      check(sf_set_ri(h_, run, ri));
+      ri_[run] = ri;
+    }
+  }
+  sf_solver* h() const { return h_; }
+  int nrun() const { return nrun_; }
+  const Params& params() const { return p_; }
+  double dt() const { return dt_; }
+
+ private:
+  Params p_;
+  int nrun_;
+  std::vector<double> ri_;
+  double dt_;
+  sf_solver* h_ = nullptr;
+};
+
+// M device states of one grid
+class Store {
+ public:
+  Store(Solver& like, int n) : n_(n) { check(sf_vecs_create(like.h(), n, &v_)); }
+  ~Store() { sf_vecs_destroy(v_); }
+  Store(const Store&) = delete;
+  Store& operator=(const Store&) = delete;
+  sf_vecs* v() const { return v_; }
+  int n() const { return n_; }
+
+ private:
+  int n_;
+  sf_vecs* v_ = nullptr;
+};
+
+// The evolution context: parameters, the segment count M and the batched
+// solver (the reference's static StateVector::solver, StateVector.h:546).
+struct Context {
+  Params p;
+  int M = 1;
+  std::unique_ptr<Solver> solver;   // nrun = M
+  std::unique_ptr<Solver> tangent;  // nrun = 2M: M bases + M tangent-linear runs
+  long long evolutions = 0;         // batched integrations performed
+  double evolve_seconds = 0;
+  Context(const Params& prm, int m) : p(prm), M(m), solver(new Solver(prm, m)) {}
+  Solver& tangent_solver() {
+    if (!tangent) {
+      tangent.reset(new Solver(p, 2 * M));
+      check(sf_set_tangent(tangent->h(), M));
+    }
+    return *tangent;
+  }
+};
+
+// Multiple-shooting state (StateVector for M = 1, plus the scalar of
+// ExtendedStateVector, ExtendedStateVector.h:6-96)
+class Vec {
+ public:
+  explicit Vec(Context& c) : c_(&c), s_(new Store(*c.solver, c.M)) {}
+  Vec(const Vec& o) : c_(o.c_), s_(new Store(*o.c_->solver, o.c_->M)), p(o.p) {
+    check(sf_vecs_copy_range(o));
+  }
+  Vec& operator=(const Vec& o) {
+    if (this != &o) {
+      check(sf_vecs_copy_range(o));
+      p = o.p;
+    }
+    return *this;
+  }
+  double p = 0.0;
+
+  int M() const { return c_->M; }
+  sf_vecs* v() const { return s_->v(); }
+  Context& ctx() const { return *c_; }
+
+  // MulAdd (StateVector.h:67-78, ExtendedStateVector.h:28-32), then EnforceBCs
+  void MulAdd(double a, const Vec& x) {
+    check(sf_vecs_axpy(v(), 0, a, x.v(), 0, M()));
+    p += a * x.p;
+    EnforceBCs();
+  }
+  Vec& operator+=(const Vec& x) { MulAdd(1.0, x); return *this; }
+  Vec& operator-=(const Vec& x) { MulAdd(-1.0, x); return *this; }
+  Vec& operator*=(double a) {
+    check(sf_vecs_scale(v(), 0, a, M()));
+    p *= a;
+    return *this;
+  }
+  // StateVector::Dot summed over the segments + p p' (ExtendedStateVector.h:12-15)
+  double Dot(const Vec& o, bool with_p = true) const {
+    double d = 0;
+    check(sf_vecs_dot_sum(v(), 0, o.v(), 0, M(), c_->p.Ri, &d));
+    return d + (with_p ? p * o.p : 0.0);
+  }
+  double Norm2() const { return Dot(*this); }
+  double Norm() const { return std::sqrt(Norm2()); }
+  void Zero() {
+    check(sf_vecs_scale(v(), 0, 0.0, M()));
+    p = 0;
+  }
+  void EnforceBCs() { check(sf_vecs_enforce_bcs(v(), 0, M())); }
+  // RemovePhaseShift of segment 0, the same shift applied to every segment
+  double RemovePhaseShift() {
+    double s = 0;
+    check(sf_vecs_phase_shift(v(), 0, 0, &s));
+    for (int i = 1; i < M(); i++) check(sf_vecs_phase_shift(v(), i, 1, &s));
+    return s;
+  }
+  void RemoveAverage(int field) {
+    for (int i = 0; i < M(); i++) check(sf_vecs_remove_average(v(), i, field, c_->p.L3));
+  }
+  void set_segment_host(int i, const float* kept) { check(sf_vecs_set_host(v(), i, kept)); }
+  void get_segment_host(int i, float* kept) const { check(sf_vecs_get_host(v(), i, kept)); }
+
+ private:
+  int sf_vecs_copy_range(const Vec& o) {
+    for (int i = 0; i < M(); i++) {
+      int rc = sf_vecs_copy(v(), i, o.v(), i);
+      if (rc) return rc;
+    }
+    return SF_OK;
+  }
+  Context* c_;
+  std::unique_ptr<Store> s_;
+};
+
+// Evolve every segment of x over tau at the given Ri (FullEvolve with a fixed
+// step, StateVector.cpp:3-84, 85-105): p is zeroed, the state projected
+// (RemoveDivergence(0)), nsteps = ceil(tau/dt) equal steps, EnforceBCs on
+// the result. If `extra` is given it receives the state one more step later
+// (for the time derivative of the flow map).
+inline void Evolve(const Vec& x, double tau, double Ri, Vec& out, Vec* extra = nullptr) {
+  Context& c = x.ctx();
+  auto t0 = std::chrono::steady_clock::now();
+  const int nsteps = std::max(1, (int)std::ceil(tau / c.p.dt - 1e-9));
+  c.solver->set_dt(tau / nsteps);
+  for (int r = 0; r < c.M; r++) c.solver->set_ri(r, Ri);
+  const double p = x.p;
+  if (&out != &x) out = x;
+  // p = 0 at the start of every integration: the map depends on u1..b only
+  check(sf_vecs_zero_pressure(out.v(), 0, c.M));
+  check(sf_vecs_to_run(out.v(), 0, c.solver->h(), 0, c.M));
+  check(sf_prepare(c.solver->h()));
+  check(sf_step(c.solver->h(), nsteps));
+  check(sf_vecs_from_run(out.v(), 0, c.solver->h(), 0, c.M));
+  if (extra) {
+    check(sf_step(c.solver->h(), 1));
+    check(sf_vecs_from_run(extra->v(), 0, c.solver->h(), 0, c.M));
+    extra->EnforceBCs();
+    extra->p = p;
+  }
+  out.EnforceBCs();
+  out.p = p;
+  check(sf_vecs_synchronize(out.v()));
+  c.evolutions += 1;
+  c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The derivative of Evolve at x applied to dx, exactly (to FP32 rounding):
+// the bases x and the perturbations dx advance together in one batch, each
+// perturbation by TimeStepLinear (IMEXRK.h:334-352) about its base's state
+// at the same RK stage. The pressure of both is zeroed and both are
+// projected first, as Evolve does; out.p = dx.p.
+inline void EvolveTangent(const Vec& x, const Vec& dx, double tau, double Ri, Vec& out) {
+  Context& c = x.ctx();
+  auto t0 = std::chrono::steady_clock::now();
+  Solver& s = c.tangent_solver();
+  const int nsteps = std::max(1, (int)std::ceil(tau / c.p.dt - 1e-9));
+  s.set_dt(tau / nsteps);
+  for (int r = 0; r < 2 * c.M; r++) s.set_ri(r, Ri);
+  const double p = dx.p;
+  Vec b(x);
+  if (&out != &dx) out = dx;
+  check(sf_vecs_zero_pressure(b.v(), 0, c.M));
+  check(sf_vecs_zero_pressure(out.v(), 0, c.M));
+  check(sf_vecs_to_run(b.v(), 0, s.h(), 0, c.M));
+  check(sf_vecs_to_run(out.v(), 0, s.h(), c.M, c.M));
+  check(sf_prepare(s.h()));
+  check(sf_step(s.h(), nsteps));
+  check(sf_vecs_from_run(out.v(), 0, s.h(), c.M, c.M));
+  out.EnforceBCs();
+  out.p = p;
+  check(sf_vecs_synchronize(out.v()));
+  c.evolutions += 1;
+  c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ------------------------------------------------------------ FP64 SVD ----
+// one-sided Jacobi SVD of an m x n matrix (m >= n), row-major A:
+// A = U diag(S) V^T, U m x n, V n x n
+inline void svd(std::vector<double> A, int m, int n, std::vector<double>& U, std::vector<double>& S,
+                std::vector<double>& V) {
+  V.assign((size_t)n * n, 0.0);
+  for (int i = 0; i < n; i++) V[(size_t)i * n + i] = 1.0;
+  for (int sweep = 0; sweep < 60; sweep++) {
+    double off = 0;
+    for (int p = 0; p < n - 1; p++)
+      for (int q = p + 1; q < n; q++) {
+        double a = 0, b = 0, d = 0;
+        for (int i = 0; i < m; i++) {
+          double x = A[(size_t)i * n + p], y = A[(size_t)i * n + q];
+          a += x * x; b += y * y; d += x * y;
+        }
+        if (std::fabs(d) <= 1e-300 || std::fabs(d) <= 1e-15 * std::sqrt(a * b)) continue;
+        off = std::max(off, std::fabs(d) / std::sqrt(a * b));
+        double zeta = (b - a) / (2 * d);
+        double t = (zeta >= 0 ? 1.0 : -1.0) / (std::fabs(zeta) + std::sqrt(1 + zeta * zeta));
+        double cs = 1 / std::sqrt(1 + t * t), sn = cs * t;
+        for (int i = 0; i < m; i++) {
+          double x = A[(size_t)i * n + p], y = A[(size_t)i * n + q];
+          A[(size_t)i * n + p] = cs * x - sn * y;
+          A[(size_t)i * n + q] = sn * x + cs * y;
+        }
+        for (int i = 0; i < n; i++) {
+          double x = V[(size_t)i * n + p], y = V[(size_t)i * n + q];
+          V[(size_t)i * n + p] = cs * x - sn * y;
+          V[(size_t)i * n + q] = sn * x + cs * y;
+        }
+      }
+    if (off < 1e-15) break;
+  }
+  S.assign(n, 0.0);
+  U.assign((size_t)m * n, 0.0);
+  for (int j = 0; j < n; j++) {
+    double s = 0;
+    for (int i = 0; i < m; i++) s += A[(size_t)i * n + j] * A[(size_t)i * n + j];
+    s = std::sqrt(s);
+    S[j] = s;
+    for (int i = 0; i < m; i++) U[(size_t)i * n + j] = s > 0 ? A[(size_t)i * n + j] / s : 0.0;
+  }
+}
+
+// ------------------------------------------------------- Newton-Krylov ----
+struct NKOptions {
+  int max_newton = 20;
+  int krylov = 80;            // GMRES basis size (K, NewtonKrylov.h:237)
+  double target = 1e-6;       // relative residual |F(x)| / |x|
+  double gmres_tol = 0.01;    // relative GMRES residual (NewtonKrylov.h:96)
+  double Delta = 100;         // initial trust region, relative to |x| (NewtonKrylov.h:29)
+  double fd_eps = 3e-4;       // finite-difference step relative to |x|
+  bool tangent = true;        // Jacobian actions by the tangent-linear batch, else by
+                              // finite differences (NewtonKrylov.h:218-235)
+};
+
+struct NKStats {
+  int newton_iterations = 0;
+  int krylov_vectors = 0;       // Jacobian actions
+  long long evolutions = 0;     // batched integrations
+  double seconds = 0;
+  double evolve_seconds = 0;
+  double residual = 0;
+  bool converged = false;
+  std::vector<double> residuals;
+};
+
+// NewtonKrylov<VectorType> (NewtonKrylov.h:1-241) with FP64 Gram-Schmidt,
+// Hessenberg and least squares, EvalDerivative by finite differences, and
+// the hookstep trust region whose acceptance test the reference leaves
+// switched off (NewtonKrylov.h:48, 69): a step is taken only if it lowers
+// the residual, otherwise Delta is halved and the constrained least-squares
+// problem is solved again in the same Krylov basis.
+class NewtonKrylov {
+ public:
+  explicit NewtonKrylov(const NKOptions& o) : opt(o) {}
+  virtual ~NewtonKrylov() = default;
+  NKOptions opt;
+
+  virtual Vec EvalFunction(const Vec& at) = 0;
+  virtual void EnforceConstraints(Vec& at) { (void)at; }
+  // called after F has been evaluated at each accepted Newton iterate
+  virtual void AtIterate(const Vec& x, const Vec& F) { (void)x; (void)F; }
+  // J * dir about the current Newton iterate (x0, F0 = F(x0))
+  virtual Vec EvalDerivative(const Vec& dir) {
+    const double eps = opt.fd_eps * x0_->Norm() / std::max(dir.Norm(), 1e-300);
+    Vec t(*x0_);
+    t.MulAdd(eps, dir);
+    Vec r = EvalFunction(t);
+    r.MulAdd(-1.0, *F0_);
+    r *= 1.0 / eps;
+    return r;
+  }
+
+  NKStats Run(Vec& x) {
+    NKStats st;
+    auto t0 = std::chrono::steady_clock::now();
+    Context& c = x.ctx();
+    const long long ev0 = c.evolutions;
+    const double es0 = c.evolve_seconds;
+    std::unique_ptr<Vec> F(new Vec(EvalFunction(x)));
+    double xn = std::max(x.Norm(), 1e-300);
+    double res = F->Norm() / xn;
+    double Delta = opt.Delta * xn;
+    st.residuals.push_back(res);
+    for (int it = 0; it < opt.max_newton && res >= opt.target; it++) {
+      x0_ = &x;
+      F0_ = F.get();
+      AtIterate(x, *F);
+      st.krylov_vectors += GMRES(*F);
+      bool accepted = false;
+      for (int attempt = 0; attempt < 8 && !accepted; attempt++) {
+        double zn = 0;
+        Vec dx = Hookstep(x, Delta, zn);
+        Vec xt(x);
+        xt.MulAdd(1.0, dx);
+        EnforceConstraints(xt);
+        EnforceConstraints(xt);
+        EnforceConstraints(xt);
+        std::unique_ptr<Vec> Ft(new Vec(EvalFunction(xt)));
+        const double rt = Ft->Norm() / std::max(xt.Norm(), 1e-300);
+        if (rt < res) {
+          x = xt;
+          F = std::move(Ft);
+          if (zn >= 0.9 * Delta && rt < 0.5 * res) Delta *= 2;   // the step hit the region and worked
+          res = rt;
+          accepted = true;
+        } else {
+          Delta = 0.5 * std::min(Delta, zn);
+        }
+      }
+      basis_.clear();
+      st.newton_iterations++;
+      st.residuals.push_back(res);
+      if (!accepted) break;
+    }
+    st.residual = res;
+    st.converged = res < opt.target;
+    st.evolutions = c.evolutions - ev0;
+    st.evolve_seconds = c.evolve_seconds - es0;
+    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    x0_ = nullptr;
+    F0_ = nullptr;
+    return st;
+  }
+
+ protected:
+  const Vec* x0_ = nullptr;
+  const Vec* F0_ = nullptr;
+  std::vector<std::unique_ptr<Vec>> basis_;
+  std::vector<double> H_;   // (K) x (K-1), row-major with stride K-1
+  double beta_ = 0;
+  int n_ = 0;               // columns of the Hessenberg block in use
+
+  // Arnoldi with modified Gram-Schmidt (NewtonKrylov.h:150-177) for A = -J
+  // until the unconstrained least-squares residual is below gmres_tol or the
+  // basis is full; keeps the basis for the hooksteps. Returns the number of
+  // Jacobian actions.
+  int GMRES(const Vec& rhs) {
+    const int K = opt.krylov;
+    basis_.clear();
+    H_.assign((size_t)K * (K - 1), 0.0);
+    basis_.emplace_back(new Vec(rhs));
+    basis_[0]->EnforceBCs();
+    beta_ = basis_[0]->Norm();
+    n_ = 0;
+    if (!(beta_ > 0)) return 0;
+    *basis_[0] *= 1.0 / beta_;
+    int used = 0;
+    for (int k = 1; k < K; k++) {
+      basis_.emplace_back(new Vec(EvalDerivative(*basis_[k - 1])));
+      *basis_[k] *= -1.0;   // factor of -1 for the Newton iteration
+      used++;
+      for (int j = 0; j < k; j++) {
+        const double h = basis_[j]->Dot(*basis_[k]);
+        H_[(size_t)j * (K - 1) + (k - 1)] = h;
+        basis_[k]->MulAdd(-h, *basis_[j]);
+      }
+      const double hn = basis_[k]->Norm();
+      H_[(size_t)k * (K - 1) + (k - 1)] = hn;
+      if (hn > 0) *basis_[k] *= 1.0 / hn;
+      basis_[k]->EnforceBCs();
+      n_ = k;
+      double zn;
+      if (LeastSquares(1e300, zn) < opt.gmres_tol || !(hn > 1e-14 * beta_)) break;
+    }
+    return used;
+  }
+
+  // min |beta e_0 - H y| with |y| <= Delta through the SVD of H (Chandler &
+  // Kerswell 2013, as NewtonKrylov.h:179-216); returns the relative residual
+  double LeastSquares(double Delta, double& znorm) {
+    const int K = opt.krylov, m = n_ + 1, n = n_;
+    std::vector<double> sub((size_t)m * n), U, S, V;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) sub[(size_t)i * n + j] = H_[(size_t)i * (K - 1) + j];
+    svd(sub, m, n, U, S, V);
+    std::vector<double> pv(n), z(n);
+    for (int j = 0; j < n; j++) pv[j] = U[j] * beta_;   // U^T (beta e_0)
+    auto zfor = [&](double mu) {
+      double s = 0;
+      for (int j = 0; j < n; j++) {
+        const double d = S[j];
+        z[j] = (d * d + mu) > 0 ? pv[j] * d / (d * d + mu) : 0.0;
+        s += z[j] * z[j];
+      }
+      return std::sqrt(s);
+    };
+    double mu = 0;
+    if (zfor(0) > Delta) {
+      double lo = 0, hi = 1e-12;
+      while (zfor(hi) > Delta) hi *= 4;
+      for (int b = 0; b < 80; b++) {
+        const double mid = 0.5 * (lo + hi);
+        (zfor(mid) > Delta ? lo : hi) = mid;
+      }
+      mu = hi;
+    }
+    znorm = zfor(mu);
+    y_.assign(n, 0.0);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) y_[i] += V[(size_t)i * n + j] * z[j];
+    double r2 = 0;
+    for (int i = 0; i < m; i++) {
+      double s = (i == 0) ? -beta_ : 0.0;
+      for (int j = 0; j < n; j++) s += sub[(size_t)i * n + j] * y_[j];
+      r2 += s * s;
+    }
+    return std::sqrt(r2) / beta_;
+  }
+
+  Vec Hookstep(const Vec& like, double Delta, double& znorm) {
+    Vec dx(like);
+    dx.Zero();
+    if (n_ == 0) {
+      znorm = 0;
+      return dx;
+    }
+    LeastSquares(Delta, znorm);
+    for (int k = 0; k < n_; k++) dx.MulAdd(y_[k], *basis_[k]);
+    return dx;
+  }
+
+  std::vector<double> y_;
+};
+
+// F_i = Phi(x_i) - x_{i+1 mod M} for every segment i
+inline Vec ShootingResidual(const Vec& phi, const Vec& at) {
+  Vec r(phi);
+  const int M = at.M();
+  for (int i = 0; i < M; i++) check(sf_vecs_axpy(r.v(), i, -1.0, at.v(), (i + 1) % M, 1));
+  r.EnforceBCs();
+  return r;
+}
+
+// Dot of segment `seg` of a and b (StateVector::Dot)
+inline double SegmentDot(const Vec& a, const Vec& b, int seg) {
+  double d = 0;
+  check(sf_vecs_dot_sum(a.v(), seg, b.v(), seg, 1, a.ctx().p.Ri, &d));
+  return d;
+}
+
+// FindPeriodic (FindPeriodic.cpp:4-28) by multiple shooting: unknowns
+// (x_0..x_{M-1}, p = T); F_i = Phi_{T/M}(x_i) - x_{i+1 mod M},
+// F_p = n . (x_0 - x_ref) with n the flow direction at the initial guess
+// (the reference uses n . (Phi_T(x) - offset)).
+class PeriodicOrbit : public NewtonKrylov {
+ public:
+  PeriodicOrbit(const NKOptions& o, const Vec& guess) : NewtonKrylov(o), ref_(guess), normal_(guess) {
+    Context& c = guess.ctx();
+    Vec e1(guess), e2(guess);
+    Evolve(guess, c.p.dt, c.p.Ri, e1, &e2);
+    normal_ = e2;
+    normal_.MulAdd(-1.0, e1);
+    normal_ *= 1.0 / c.p.dt;
+    normal_.p = 0;
+  }
+  Vec EvalFunction(const Vec& at) override {
+    Context& c = at.ctx();
+    Vec phi(at), ext(at);
+    Evolve(at, at.p / c.M, c.p.Ri, phi, &ext);
+    Vec r = ShootingResidual(phi, at);
+    Vec d(at);
+    d.MulAdd(-1.0, ref_);
+    r.p = SegmentDot(normal_, d, 0);
+    ext.MulAdd(-1.0, phi);   // flow direction at the segment ends
+    ext *= 1.0 / c.solver->dt();
+    last_f_.reset(new Vec(ext));
+    return r;
+  }
+  void AtIterate(const Vec& x, const Vec& F) override {
+    (void)x; (void)F;
+    f0_ = std::move(last_f_);
+  }
+  // J (dX, dT): Phi' dx_i - dx_{i+1}, plus dT/M times the flow direction at
+  // the segment ends, and the phase condition n . dx_0
+  Vec EvalDerivative(const Vec& dir) override {
+    Vec d(dir);
+    d.p = 0;
+    Vec r(d);
+    if (opt.tangent) {
+      Context& c = d.ctx();
+      Vec phi(d);
+      EvolveTangent(*x0_, d, x0_->p / c.M, c.p.Ri, phi);
+      r = ShootingResidual(phi, d);
+    } else {
+      r = NewtonKrylov::EvalDerivative(d);
+    }
+    if (f0_) r.MulAdd(dir.p / dir.ctx().M, *f0_);
+    r.p = SegmentDot(normal_, d, 0);
+    return r;
+  }
+
+ private:
+  Vec ref_, normal_;
+  std::unique_ptr<Vec> last_f_, f0_;
+};
+
+// PseudoArclengthContinuation (PseudoArclength.h:6-42) by multiple shooting:
+// unknowns (x_0..x_{M-1}, p = Ri); F_i = Phi_{T/M}(x_i; Ri) - x_{i+1 mod M},
+// F_p = ds - v . (X - X0); EnforceConstraints removes the phase shift and the
+// averages of u1 and b (PseudoArclength.h:15-20).
+class PseudoArclength : public NewtonKrylov {
+ public:
+  PseudoArclength(const NKOptions& o, const Vec& x0, const Vec& v, double ds, double T)
+      : NewtonKrylov(o), x0c_(x0), v_(v), ds_(ds), T_(T) {}
+  Vec EvalFunction(const Vec& at) override {
+    Context& c = at.ctx();
+    Vec phi(at);
+    Evolve(at, T_ / c.M, at.p, phi);
+    Vec r = ShootingResidual(phi, at);
+    Vec d(at);
+    d.MulAdd(-1.0, x0c_);
+    r.p = ds_ - v_.Dot(d);
+    last_phi_.reset(new Vec(phi));
+    return r;
+  }
+  void EnforceConstraints(Vec& at) override {
+    at.RemovePhaseShift();
+    at.RemoveAverage(0);
+    at.RemoveAverage(3);
+  }
+  // dPhi/dRi at the Newton iterate by a one-sided difference in Ri
+  void AtIterate(const Vec& x, const Vec& F) override {
+    (void)F;
+    if (!opt.tangent || !last_phi_) return;
+    const double e = std::max(1e-3 * std::fabs(x.p), 1e-5);
+    Vec phi(x);
+    Evolve(x, T_ / x.ctx().M, x.p + e, phi);
+    phi.MulAdd(-1.0, *last_phi_);
+    phi *= 1.0 / e;
+    phi.p = 0;
+    dphi_dri_.reset(new Vec(phi));
+  }
+  // J (dX, dRi) = Phi' dx_i + dRi dPhi/dRi - dx_{i+1}; -v . (dX, dRi)
+  Vec EvalDerivative(const Vec& dir) override {
+    if (!opt.tangent || !dphi_dri_) return NewtonKrylov::EvalDerivative(dir);
+    Vec d(dir);
+    d.p = 0;
+    Vec phi(d);
+    EvolveTangent(*x0_, d, T_ / d.ctx().M, x0_->p, phi);
+    Vec r = ShootingResidual(phi, d);
+    r.MulAdd(dir.p, *dphi_dri_);
+    r.p = -v_.Dot(dir);
+    return r;
+  }
+
+ private:
+  Vec x0c_, v_;
+  double ds_, T_;
+  std::unique_ptr<Vec> last_phi_, dphi_dri_;
+};
+
+}  // namespace stratiflow
