@@ -173,7 +173,9 @@ int sf_remove_divergence_noalloc(const sf_grid* grid, const sf_flow* flow, doubl
  * layout [5][N3][plane] (u1,u2,u3,b,p), and shares the stream of the solver
  * it was created from. Reductions accumulate in FP64. These are the Krylov
  * bases and iterates of the Newton-Krylov, Arnoldi and continuation drivers,
- * which in the reference are host std::vector<StateVector> (NewtonKrylov.h:239). */
+ * which in the reference are host std::vector<StateVector> (NewtonKrylov.h:239).
+ * Once the solver is destroyed, sf_vecs_destroy is the only valid call on
+ * its stores. */
 typedef struct sf_vecs sf_vecs;
 int sf_vecs_create(sf_solver* like, int nvec, sf_vecs** out);
 int sf_vecs_destroy(sf_vecs* v);
@@ -205,9 +207,45 @@ int sf_vecs_enforce_bcs(sf_vecs* v, int i, int count);
 int sf_vecs_phase_shift(sf_vecs* v, int i, int use_given, double* shift);
 /* RemoveAverage (Integration.h:236-240) of field 0 (u1) or 3 (b) */
 int sf_vecs_remove_average(sf_vecs* v, int i, int field, double L3);
+/* Block operations of the block Krylov solvers (nb <= 32), FP64 sums:
+ * out[i*nb + k] = Dot(v[a+i], w[b+k]) for i < na, k < nb */
+int sf_vecs_gram(sf_vecs* v, int a, int na, sf_vecs* w, int b, int nb, double Ri, double* out);
+/* w[b+k] += alpha * sum_i coef[i*nb + k] v[a+i] on u1..b (coef host, na x nb;
+ * the two ranges must not overlap) */
+int sf_vecs_update(sf_vecs* w, int b, int nb, double alpha, sf_vecs* v, int a, int na, const double* coef);
+/* keep only the fields of field_mask (bit 0 u1, 1 u2, 2 u3, 3 b) and the
+ * modes with j1_lo <= j1 < j1_hi in vector i; p is zeroed */
+int sf_vecs_band(sf_vecs* v, int i, int field_mask, int j1_lo, int j1_hi);
 /* zero the p field of vectors i..i+count-1 */
 int sf_vecs_zero_pressure(sf_vecs* v, int i, int count);
 int sf_vecs_synchronize(sf_vecs* v);
+
+/* ---- learned continuation predictor (no counterpart in the reference; it
+ * stands beside the secant predictor of PseudoArclength.cpp:33-61) ----
+ * nlayers 1D convolutions along z (5 taps, zero padding 2) with ReLU between
+ * them; channels[0] inputs, channels[nlayers] outputs, each a multiple of 8.
+ * Tensors are FP32 on the host, channel-last [batch][Z][C]; on the device
+ * the operands are BF16 and the tensor-core contractions accumulate in FP32.
+ * Parameters, FP32: for each layer W[Cout][5][Cin] then bias[Cout]. The
+ * weights start He-normal from `seed`, the output layer at zero. stream is
+ * a cudaStream_t (NULL: legacy default stream). */
+typedef struct sf_net sf_net;
+int sf_net_create(int nlayers, const int* channels, int Z, int max_batch, unsigned long long seed, void* stream,
+                  sf_net** out);
+int sf_net_destroy(sf_net* n);
+int sf_net_num_params(sf_net* n, long long* count);
+int sf_net_get_params(sf_net* n, float* host);
+/* also resets the Adam moments */
+int sf_net_set_params(sf_net* n, const float* host);
+/* y[batch][Z][Cout] = net(x[batch][Z][Cin]); discards the training data */
+int sf_net_forward(sf_net* n, const float* x, int batch, float* y);
+/* uploads a training set: inputs x[batch][Z][Cin], targets [batch][Z][Cout] */
+int sf_net_set_data(sf_net* n, const float* x, const float* target, int batch);
+/* mean-square loss over the training set and its gradient (parameter layout) */
+int sf_net_gradient(sf_net* n, float* grad, double* loss);
+/* `steps` full-batch Adam steps (lr; beta 0.9, 0.999; eps 1e-8); losses[s]
+ * (may be NULL) is the loss before step s */
+int sf_net_train(sf_net* n, int steps, double lr, double* losses);
 
 /* waits for all work queued on the solver's stream */
 int sf_synchronize(sf_solver* s);

@@ -34,6 +34,9 @@ EXPORTS = [
     "sf_vecs_copy", "sf_vecs_set_host", "sf_vecs_get_host", "sf_vecs_axpy", "sf_vecs_lincomb", "sf_vecs_scale",
     "sf_vecs_dots", "sf_vecs_dot_sum", "sf_vecs_enforce_bcs", "sf_vecs_phase_shift", "sf_vecs_remove_average",
     "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
+    "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
+    "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
+    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band",
 ]
 
 
@@ -84,6 +87,12 @@ def load_library(path: str | None = None):
         "sf_vecs_dot_sum": [vp, i, vp, i, i, d, dp], "sf_vecs_enforce_bcs": [vp, i, i],
         "sf_vecs_phase_shift": [vp, i, i, dp], "sf_vecs_remove_average": [vp, i, i, d], "sf_vecs_synchronize": [vp],
         "sf_vecs_zero_pressure": [vp, i, i], "sf_set_tangent": [vp, i],
+        "sf_net_create": [i, C.POINTER(i), i, i, C.c_ulonglong, vp, C.POINTER(vp)], "sf_net_destroy": [vp],
+        "sf_net_num_params": [vp, C.POINTER(C.c_longlong)], "sf_net_get_params": [vp, fp],
+        "sf_net_set_params": [vp, fp], "sf_net_forward": [vp, fp, i, fp], "sf_net_set_data": [vp, fp, fp, i],
+        "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
+        "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
+        "sf_vecs_band": [vp, i, i, i, i],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -344,6 +353,20 @@ class Vecs:
     def remove_average(self, i, field, L3):
         _check(load_library().sf_vecs_remove_average(self._h, int(i), int(field), float(L3)))
 
+    def gram(self, a, na, other: "Vecs", b, nb, Ri):
+        out = np.zeros((int(na), int(nb)))
+        _check(load_library().sf_vecs_gram(self._h, int(a), int(na), other._h, int(b), int(nb), float(Ri),
+                                           out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def update(self, b, nb, alpha, other: "Vecs", a, na, coef):
+        coef = np.ascontiguousarray(coef, dtype=np.float64).reshape(int(na), int(nb))
+        _check(load_library().sf_vecs_update(self._h, int(b), int(nb), float(alpha), other._h, int(a), int(na),
+                                             coef.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def band(self, i, field_mask, j1_lo, j1_hi):
+        _check(load_library().sf_vecs_band(self._h, int(i), int(field_mask), int(j1_lo), int(j1_hi)))
+
     def zero_pressure(self, i, count=1):
         _check(load_library().sf_vecs_zero_pressure(self._h, int(i), int(count)))
 
@@ -351,5 +374,65 @@ class Vecs:
         _check(load_library().sf_vecs_synchronize(self._h))
 
 
-__all__ = ["IMEXRK", "Vecs", "SFError", "load_library", "EXPORTS", "vertical_points",
+class Net:
+    """The convolutional continuation predictor (sf_net_*): `channels` has
+    nlayers + 1 entries; tensors are float32 [batch][Z][C]."""
+
+    def __init__(self, channels, Z, max_batch, seed=0, stream=None):
+        self.channels = [int(c) for c in channels]
+        self.Z, self.max_batch = int(Z), int(max_batch)
+        ch = (C.c_int * len(self.channels))(*self.channels)
+        self._h = C.c_void_p()
+        _check(load_library().sf_net_create(len(self.channels) - 1, ch, self.Z, self.max_batch, int(seed),
+                                            C.c_void_p(stream), C.byref(self._h)))
+        n = C.c_longlong()
+        _check(load_library().sf_net_num_params(self._h, C.byref(n)))
+        self.num_params = n.value
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and h.value:
+            load_library().sf_net_destroy(h)
+            self._h = C.c_void_p()
+
+    def get_params(self):
+        out = np.zeros(self.num_params, dtype=np.float32)
+        _check(load_library().sf_net_get_params(self._h, _fptr(out)))
+        return out
+
+    def set_params(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        assert w.size == self.num_params
+        _check(load_library().sf_net_set_params(self._h, _fptr(w)))
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        B = x.shape[0]
+        assert x.shape == (B, self.Z, self.channels[0])
+        y = np.zeros((B, self.Z, self.channels[-1]), dtype=np.float32)
+        _check(load_library().sf_net_forward(self._h, _fptr(x), B, _fptr(y)))
+        return y
+
+    def set_data(self, x, target):
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        target = np.ascontiguousarray(target, dtype=np.float32)
+        B = x.shape[0]
+        assert x.shape == (B, self.Z, self.channels[0]) and target.shape == (B, self.Z, self.channels[-1])
+        self._data = (x, target)   # the host arrays outlive the asynchronous upload
+        _check(load_library().sf_net_set_data(self._h, _fptr(x), _fptr(target), B))
+
+    def gradient(self):
+        g = np.zeros(self.num_params, dtype=np.float32)
+        loss = C.c_double()
+        _check(load_library().sf_net_gradient(self._h, _fptr(g), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, steps, lr):
+        losses = np.zeros(int(steps))
+        _check(load_library().sf_net_train(self._h, int(steps), float(lr),
+                                           losses.ctypes.data_as(C.POINTER(C.c_double))))
+        return losses
+
+
+__all__ = ["IMEXRK", "Vecs", "Net", "SFError", "load_library", "EXPORTS", "vertical_points",
            "vertical_points_fractional", "neumann_profile", "background_profile", "kept_modes"]

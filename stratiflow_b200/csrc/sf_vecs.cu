@@ -4,6 +4,7 @@
 // whose Krylov bases live on the device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -27,6 +28,8 @@ struct sf_vecs {
   float2* d = nullptr;      // [nvec][5][N3][Pp]
   double* red = nullptr;    // reduction scratch
   int cap_red = 0;
+  double* coef = nullptr;   // block-update coefficients
+  size_t cap_coef = 0;
   const float* zc = nullptr;
   cudaStream_t st = nullptr;
   std::vector<double> z, zf;
@@ -91,6 +94,110 @@ __global__ void k_dots(Geo g, const float2* __restrict__ base, size_t stride, co
     const double wz = zc[(f == 2 ? ZC_WZD : ZC_WZN) * g.N3 + j];
     const double wf = (f == 3) ? wb : 1.0;
     if (wz != 0.0) atomicAdd(out + (sum ? 0 : k), t * wz * wf);
+  }
+}
+
+// Block Gram matrix: part[c][i][k] = the share of level chunk c (kGramLevels
+// levels of one field) of Dot(V_i, W_k), i < nv, k < nw <= kMaxBlock. One
+// warp per (chunk, field, i): lanes stride over the modes and keep one FP64
+// sum per k; the partial sums are added in a fixed order afterwards.
+constexpr int kGramLevels = 8;
+constexpr int kMaxBlock = 32;
+
+template <int NW>
+__global__ void __launch_bounds__(256) k_gram(Geo g, const float2* __restrict__ V, int nv,
+                                               const float2* __restrict__ W, int nw, size_t stride,
+                                               const float* __restrict__ zc, double Ri, double* __restrict__ part) {
+  const int chunk = blockIdx.x, f = blockIdx.y, warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.z * 8 + warp;
+  if (i >= nv) return;
+  const int nch = gridDim.x;
+  double acc[NW];
+#pragma unroll
+  for (int k = 0; k < NW; k++) acc[k] = 0.0;
+  if (f != 1 || g.dim3) {
+    for (int j = chunk * kGramLevels; j < min(g.N3, (chunk + 1) * kGramLevels); j++) {
+      const double wz = (double)zc[(f == 2 ? ZC_WZD : ZC_WZN) * g.N3 + j] * (f == 3 ? Ri : 1.0);
+      if (wz == 0.0) continue;
+      const size_t row = ((size_t)f * g.N3 + j) * g.Pp;
+      const float2* v = V + (size_t)i * stride + row;
+      for (int m = lane; m < g.P; m += 32) {
+        const float2 a = v[m];
+        const double wm = (m == 0) ? wz : 2.0 * wz;
+#pragma unroll
+        for (int k = 0; k < NW; k++) {
+          if (k < nw) {
+            const float2 b = W[(size_t)k * stride + row + m];
+            acc[k] += wm * ((double)a.x * b.x + (double)a.y * b.y);
+          }
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < NW; k++) {
+    double t = acc[k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    acc[k] = t;
+  }
+  if (lane == 0) {
+    double* out = part + (((size_t)f * nch + chunk) * nv + i) * nw;
+#pragma unroll
+    for (int k = 0; k < NW; k++)
+      if (k < nw) out[k] = acc[k];
+  }
+}
+
+// out[i][k] = sum over the 4 * nch partials, in order
+__global__ void k_gram_sum(const double* __restrict__ part, int nparts, int nvw, double* __restrict__ out) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nvw) return;
+  double s = 0.0;
+  for (int c = 0; c < nparts; c++) s += part[(size_t)c * nvw + e];
+  out[e] = s;
+}
+
+// W_k += alpha sum_i coef[i][k] V_i over u1,u2,u3,b, k < nw <= kMaxBlock
+template <int NW>
+__global__ void k_update(Geo g, float2* __restrict__ W, int nw, const float2* __restrict__ V, int nv, size_t stride,
+                         const double* __restrict__ coef, double alpha) {
+  const size_t n = (size_t)4 * g.fblk;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    float2 acc[NW];
+#pragma unroll
+    for (int k = 0; k < NW; k++) acc[k] = make_float2(0.f, 0.f);
+    for (int i = 0; i < nv; i++) {
+      const float2 v = V[(size_t)i * stride + e];
+      const double* c = coef + (size_t)i * nw;
+#pragma unroll
+      for (int k = 0; k < NW; k++) {
+        if (k < nw) {
+          const float ck = (float)(alpha * c[k]);
+          acc[k].x += ck * v.x;
+          acc[k].y += ck * v.y;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+      if (k < nw) {
+        float2& w = W[(size_t)k * stride + e];
+        w = make_float2(w.x + acc[k].x, w.y + acc[k].y);
+      }
+    }
+  }
+}
+
+// keep field f of mode m only if bit f of fieldmask is set and lo <= j1 < hi;
+// p is zeroed
+__global__ void k_band(Geo g, float2* v, int fieldmask, int lo, int hi) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= g.Pp) return;
+  const int j1 = m % g.K1;
+  for (int f = 0; f < 5; f++) {
+    const bool keep = f < 4 && ((fieldmask >> f) & 1) && j1 >= lo && j1 < hi && m < g.P;
+    if (keep) continue;
+    for (int j = 0; j < g.N3; j++) v[((size_t)f * g.N3 + j) * g.Pp + m] = make_float2(0.f, 0.f);
   }
 }
 
@@ -166,9 +273,11 @@ int sf_vecs_create(sf_solver* like, int nvec, sf_vecs** out) {
 
 int sf_vecs_destroy(sf_vecs* v) {
   if (!v) return SF_OK;
-  cudaStreamSynchronize(v->st);
+  // no use of the solver's stream here: the solver may be gone already;
+  // cudaFree waits for the device work that may still read the memory
   cudaFree(v->d);
   cudaFree(v->red);
+  cudaFree(v->coef);
   delete v;
   return SF_OK;
 }
@@ -332,6 +441,74 @@ int sf_vecs_remove_average(sf_vecs* v, int i, int field, double L3) {
   for (int k = 1; k < g.N3 - 1; k++) integ += (v->z[k + 1] - v->z[k]) * (double)col[k].x;
   const float value = (float)(integ / L3 / 2);
   k_sub_mean<<<(g.N3 + 127) / 128, 128, 0, v->st>>>(g, v->d + (size_t)i * vstride(g), field, value);
+  VCK(cudaGetLastError());
+  return SF_OK;
+}
+
+// out[i * nb + k] = Dot(v[a + i], w[b + k]) (StateVector::Dot, FP64)
+int sf_vecs_gram(sf_vecs* v, int a, int na, sf_vecs* w, int b, int nb, double Ri, double* out) {
+  if (!v || !w || !out || na < 1 || nb < 1 || nb > kMaxBlock || a < 0 || a + na > v->nvec || b < 0 ||
+      b + nb > w->nvec)
+    return vfail(SF_EINVAL, "bad argument (1 <= nb <= 32)");
+  const Geo& g = v->g;
+  const int nch = (g.N3 + kGramLevels - 1) / kGramLevels;
+  const size_t nvw = (size_t)na * nb, parts = (size_t)4 * nch;
+  int rc = ensure_red(v, (int)(nvw * (parts + 1)));
+  if (rc) return rc;
+  double* part = v->red + nvw;
+  dim3 grid(nch, 4, (na + 7) / 8);
+  auto* wd = w->d + (size_t)b * vstride(w->g);
+  auto* vd = v->d + (size_t)a * vstride(g);
+  const size_t vs = vstride(g);
+  if (nb <= 1) k_gram<1><<<grid, 256, 0, v->st>>>(g, vd, na, wd, nb, vs, v->zc, Ri, part);
+  else if (nb <= 4) k_gram<4><<<grid, 256, 0, v->st>>>(g, vd, na, wd, nb, vs, v->zc, Ri, part);
+  else if (nb <= 8) k_gram<8><<<grid, 256, 0, v->st>>>(g, vd, na, wd, nb, vs, v->zc, Ri, part);
+  else if (nb <= 16) k_gram<16><<<grid, 256, 0, v->st>>>(g, vd, na, wd, nb, vs, v->zc, Ri, part);
+  else k_gram<32><<<grid, 256, 0, v->st>>>(g, vd, na, wd, nb, vs, v->zc, Ri, part);
+  VCK(cudaGetLastError());
+  k_gram_sum<<<(unsigned)((nvw + 255) / 256), 256, 0, v->st>>>(part, (int)parts, (int)nvw, v->red);
+  VCK(cudaGetLastError());
+  VCK(cudaMemcpyAsync(out, v->red, sizeof(double) * nvw, cudaMemcpyDeviceToHost, v->st));
+  VCK(cudaStreamSynchronize(v->st));
+  return SF_OK;
+}
+
+// w[b + k] += alpha sum_i coef[i * nb + k] v[a + i] on u1..b (v and w ranges
+// must not overlap)
+int sf_vecs_update(sf_vecs* w, int b, int nb, double alpha, sf_vecs* v, int a, int na, const double* coef) {
+  if (!v || !w || !coef || na < 1 || nb < 1 || nb > kMaxBlock || a < 0 || a + na > v->nvec || b < 0 ||
+      b + nb > w->nvec)
+    return vfail(SF_EINVAL, "bad argument (1 <= nb <= 32)");
+  if (v == w && a < b + nb && b < a + na) return vfail(SF_EINVAL, "overlapping ranges");
+  const size_t nc = (size_t)na * nb;
+  if (nc > w->cap_coef) {
+    cudaFree(w->coef);
+    w->coef = nullptr;
+    w->cap_coef = 0;
+    VCK(cudaMalloc(&w->coef, sizeof(double) * nc));
+    w->cap_coef = nc;
+  }
+  VCK(cudaMemcpyAsync(w->coef, coef, sizeof(double) * nc, cudaMemcpyHostToDevice, w->st));
+  const Geo& g = w->g;
+  const size_t n = (size_t)4 * g.fblk;
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 4096);
+  const size_t vs = vstride(g);
+  float2* wd = w->d + (size_t)b * vs;
+  const float2* vd = v->d + (size_t)a * vs;
+  if (nb <= 1) k_update<1><<<blocks, 256, 0, w->st>>>(g, wd, nb, vd, na, vs, w->coef, alpha);
+  else if (nb <= 4) k_update<4><<<blocks, 256, 0, w->st>>>(g, wd, nb, vd, na, vs, w->coef, alpha);
+  else if (nb <= 8) k_update<8><<<blocks, 256, 0, w->st>>>(g, wd, nb, vd, na, vs, w->coef, alpha);
+  else if (nb <= 16) k_update<16><<<blocks, 256, 0, w->st>>>(g, wd, nb, vd, na, vs, w->coef, alpha);
+  else k_update<32><<<blocks, 256, 0, w->st>>>(g, wd, nb, vd, na, vs, w->coef, alpha);
+  VCK(cudaGetLastError());
+  return SF_OK;
+}
+
+// keep only the fields in field_mask (bit f: u1, u2, u3, b) and the modes
+// with j1_lo <= j1 < j1_hi of vector i; p is zeroed
+int sf_vecs_band(sf_vecs* v, int i, int field_mask, int j1_lo, int j1_hi) {
+  if (!v || i < 0 || i >= v->nvec) return vfail(SF_EINVAL, "bad argument");
+  k_band<<<(v->g.Pp + 127) / 128, 128, 0, v->st>>>(v->g, v->d + (size_t)i * vstride(v->g), field_mask, j1_lo, j1_hi);
   VCK(cudaGetLastError());
   return SF_OK;
 }

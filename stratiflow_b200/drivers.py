@@ -62,13 +62,25 @@ class Flow:
 
 class NKOptions:
     """jacobian: "tangent" (exact actions by the tangent-linear batch) or
-    "fd" (finite differences with step fd_eps |x|, NewtonKrylov.h:218-235)."""
+    "fd" (finite differences with step fd_eps |x|, NewtonKrylov.h:218-235).
+    block: directions per batched Jacobian action of the block Krylov solver
+    (single shooting, M = 1); 0 selects the one-direction solver, which also
+    runs multiple shooting. krylov: basis vectors before the solve stops."""
 
     def __init__(self, max_newton=20, krylov=80, target=1e-6, gmres_tol=0.01, Delta=100.0, fd_eps=3e-4,
-                 jacobian="tangent"):
+                 jacobian="tangent", block=16):
         assert jacobian in ("tangent", "fd")
-        self.v = np.array([max_newton, krylov, target, gmres_tol, Delta, fd_eps, 0.0 if jacobian == "tangent" else 1.0],
-                          dtype=np.float64)
+        self.v = np.array([max_newton, krylov, target, gmres_tol, Delta, fd_eps,
+                           0.0 if jacobian == "tangent" else 1.0, block], dtype=np.float64)
+
+
+def _opts(opts, M):
+    """The options as passed: multiple shooting (M > 1) runs the
+    one-direction solver."""
+    v = (opts or NKOptions()).v.copy()
+    if M > 1:
+        v[7] = 0
+    return v
 
 
 def _dp(a):
@@ -89,9 +101,12 @@ def _segments(flow, x, M):
 
 def _stats(st):
     n = int(st[7])
+    ng = max(0, min(n - 1, (len(st) - 8 - n) // 2))
+    g = st[8 + n:8 + n + 2 * ng]
     return {"newton_iterations": int(st[0]), "jacobian_actions": int(st[1]), "integrations": int(st[2]),
             "seconds": float(st[3]), "integration_seconds": float(st[4]), "residual": float(st[5]),
-            "converged": bool(st[6] > 0.5), "residuals": [float(v) for v in st[8:8 + n]]}
+            "converged": bool(st[6] > 0.5), "residuals": [float(v) for v in st[8:8 + n]],
+            "gmres_residuals": [float(v) for v in g[0::2]], "gmres_vectors": [int(v) for v in g[1::2]]}
 
 
 def _call(rc):
@@ -106,9 +121,9 @@ def newton_fixed(flow: Flow, x, T, M=1, opts: NKOptions | None = None, constrain
     L = load_host()
     xs = _segments(flow, x, M)
     out = np.zeros_like(xs)
-    st = np.zeros(8 + 64)
-    opts = opts or NKOptions()
-    _call(L.sfh_newton_fixed(_dp(flow.array()), M, float(T), int(constrain), _fp(xs), _dp(opts.v), _fp(out),
+    st = np.zeros(8 + 3 * 64)
+    ov = _opts(opts, M)
+    _call(L.sfh_newton_fixed(_dp(flow.array()), M, float(T), int(constrain), _fp(xs), _dp(ov), _fp(out),
                              _dp(st), len(st)))
     return out, _stats(st)
 
@@ -120,9 +135,9 @@ def periodic_orbit(flow: Flow, x, T0, M=16, opts: NKOptions | None = None):
     xs = _segments(flow, x, M)
     out = np.zeros_like(xs)
     T = C.c_double()
-    st = np.zeros(8 + 64)
-    opts = opts or NKOptions()
-    _call(L.sfh_periodic_orbit(_dp(flow.array()), M, float(T0), _fp(xs), _dp(opts.v), _fp(out), C.byref(T),
+    st = np.zeros(8 + 3 * 64)
+    ov = _opts(opts, M)
+    _call(L.sfh_periodic_orbit(_dp(flow.array()), M, float(T0), _fp(xs), _dp(ov), _fp(out), C.byref(T),
                                _dp(st), len(st)))
     return out, T.value, _stats(st)
 
@@ -134,10 +149,10 @@ def arclength_correct(flow: Flow, x0, Ri0, v, vRi, ds, guess, Ri_guess, T, M=1, 
     X0, V, G = (_segments(flow, a, M) for a in (x0, v, guess))
     out = np.zeros_like(G)
     ri = C.c_double()
-    st = np.zeros(8 + 64)
-    opts = opts or NKOptions()
+    st = np.zeros(8 + 3 * 64)
+    ov = _opts(opts, M)
     _call(L.sfh_arclength(_dp(flow.array()), M, float(T), _fp(X0), float(Ri0), _fp(V), float(vRi), float(ds),
-                          _fp(G), float(Ri_guess), _dp(opts.v), _fp(out), C.byref(ri), _dp(st), len(st)))
+                          _fp(G), float(Ri_guess), _dp(ov), _fp(out), C.byref(ri), _dp(st), len(st)))
     return out, ri.value, _stats(st)
 
 
@@ -211,24 +226,35 @@ def secant_predictor(flow: Flow, p1, p2, ds):
     return (guess[0].astype(np.complex64), guess[1]), (v[0].astype(np.complex64), v[1])
 
 
-def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, predictor=None, log=None):
+def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, predictor=None, log=None,
+                 fallback_after=6):
     """Pseudo-arclength continuation from two converged points
     ((x, Ri), (x, Ri)). `predictor(history, ds)` may replace the secant: it
     gets the converged points so far and returns a guess (x, Ri); the secant
-    tangent is always used for the arclength constraint. Returns the points
-    and the per-point statistics."""
+    tangent is always used for the arclength constraint. A learned guess
+    gets `fallback_after` Newton iterations; if it has not converged by then
+    the point is solved again from the secant guess. Returns the points and
+    the per-point statistics."""
     pts = list(start_points)
     stats = []
+    opts = opts or NKOptions()
     for k in range(npoints):
         t0 = time.perf_counter()
         sec_guess, (vx, vp) = secant_predictor(flow, pts[-2], pts[-1], ds)
         guess = predictor(pts, ds) if predictor is not None else sec_guess
         used = "learned" if predictor is not None else "secant"
-        x, Ri, st = arclength_correct(flow, pts[-1][0], pts[-1][1], vx, vp, ds, guess[0], guess[1], T, M, opts)
+        o = opts
+        if predictor is not None:
+            o = NKOptions()
+            o.v = opts.v.copy()
+            o.v[0] = min(opts.v[0], fallback_after)
+        x, Ri, st = arclength_correct(flow, pts[-1][0], pts[-1][1], vx, vp, ds, guess[0], guess[1], T, M, o)
         if not st["converged"] and predictor is not None:
             # the secant predictor remains the fallback
             x, Ri, st2 = arclength_correct(flow, pts[-1][0], pts[-1][1], vx, vp, ds, sec_guess[0], sec_guess[1],
                                            T, M, opts)
+            for key in ("newton_iterations", "jacobian_actions", "integrations", "seconds", "integration_seconds"):
+                st2[key] += st[key]
             st2["fallback_from"] = st
             st = st2
             used = "secant (fallback)"
@@ -242,3 +268,84 @@ def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, 
         if not st["converged"]:
             break
     return pts, stats
+
+
+# ------------------------------------------------------- learned predictor
+class LearnedPredictor:
+    """The convolutional predictor of the next branch point (sf_net, BF16
+    operands and FP32 accumulation on the tensor cores), used in place of the
+    secant guess of PseudoArclength.cpp:60-61 with the secant as fallback.
+
+    Features along z (the convolution axis), per level: the real and
+    imaginary parts of the kept modes of u1, u3 and b of the last converged
+    state and of its difference from the one before, plus the step ds and Ri
+    as constant channels. The network predicts the correction that takes the
+    secant guess to the converged point, in units of its training RMS. 2D
+    only (one kept wavenumber row)."""
+
+    def __init__(self, flow: Flow, hidden=256, layers=4, seed=0, max_batch=64):
+        from . import Net
+        assert flow.N2 == 1, "the learned predictor is 2D"
+        self.flow = flow
+        self.P = flow.N1 // 3
+        self.fields = (0, 2, 3)
+        self.nc = len(self.fields) * self.P * 2
+        self.cin = (2 * self.nc + 2 + 7) // 8 * 8
+        self.cout = (self.nc + 7) // 8 * 8
+        self.channels = [self.cin] + [hidden] * (layers - 1) + [self.cout]
+        self.net = Net(self.channels, flow.N3, max_batch, seed=seed)
+        self.scale = None
+        self.losses = None
+
+    def _feat(self, x):
+        x = np.asarray(x).reshape(self.flow.state_shape)
+        sel = x[list(self.fields), :, :self.P]
+        f = np.stack([sel.real, sel.imag], axis=-1)            # [field][z][mode][re|im]
+        return f.transpose(1, 0, 2, 3).reshape(self.flow.N3, self.nc).astype(np.float64)
+
+    def _unfeat(self, f):
+        x = np.zeros(self.flow.state_shape, dtype=np.complex128)
+        g = f.reshape(self.flow.N3, len(self.fields), self.P, 2).transpose(1, 0, 2, 3)
+        for i, fld in enumerate(self.fields):
+            x[fld, :, :self.P] = g[i, ..., 0] + 1j * g[i, ..., 1]
+        return x
+
+    def _inputs(self, p1, p2, ds):
+        (x1, r1), (x2, r2) = p1, p2
+        a, b = self._feat(x2), self._feat(x2) - self._feat(x1)
+        sx, sd, sds, sri = self.scale["x"], self.scale["d"], self.scale["ds"], self.scale["Ri"]
+        out = np.zeros((self.flow.N3, self.cin), dtype=np.float32)
+        out[:, :self.nc] = a / sx
+        out[:, self.nc:2 * self.nc] = b / sd
+        out[:, 2 * self.nc] = ds / sds
+        out[:, 2 * self.nc + 1] = r2 / sri
+        return out
+
+    def fit(self, points, ds, steps=1500, lr=1e-3):
+        """Train on consecutive triples of converged points (x, Ri): inputs
+        from the first two, target = third - secant guess. Returns the
+        losses."""
+        triples = [(points[k - 2], points[k - 1], points[k]) for k in range(2, len(points))]
+        assert triples, "need at least three converged points"
+        feats = [self._feat(p[0]) for p in points]
+        diffs = [feats[k] - feats[k - 1] for k in range(1, len(points))]
+        tg = []
+        for p1, p2, p3 in triples:
+            (gx, _), _ = secant_predictor(self.flow, p1, p2, ds)
+            tg.append(self._feat(p3[0]) - self._feat(gx))
+        rms = lambda arrs: float(np.sqrt(np.mean([np.mean(a ** 2) for a in arrs]))) or 1.0
+        self.scale = {"x": rms(feats), "d": rms(diffs), "t": rms(tg), "ds": abs(ds) or 1.0,
+                      "Ri": max(abs(p[1]) for p in points) or 1.0}
+        X = np.stack([self._inputs(p1, p2, ds) for p1, p2, _ in triples])
+        Y = np.zeros((len(triples), self.flow.N3, self.cout), dtype=np.float32)
+        for i, t in enumerate(tg):
+            Y[i, :, :self.nc] = t / self.scale["t"]
+        self.net.set_data(X, Y)
+        self.losses = self.net.train(steps, lr)
+        return self.losses
+
+    def __call__(self, pts, ds):
+        sec_guess, _ = secant_predictor(self.flow, pts[-2], pts[-1], ds)
+        y = self.net.forward(self._inputs(pts[-2], pts[-1], ds)[None])[0]
+        corr = self._unfeat(y[:, :self.nc].astype(np.float64) * self.scale["t"])
+        return (sec_guess[0] + corr).astype(np.complex64), sec_guess[1]

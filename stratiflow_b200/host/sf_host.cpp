@@ -38,6 +38,10 @@ NKOptions options_from(const double* o) {
   return n;
 }
 
+// directions per batched Jacobian action of the block solver (opts[7]); 0
+// selects the one-direction solver
+int block_from(const double* o) { return o ? (int)o[7] : 0; }
+
 size_t kept_elems(const Params& p) {
   const int K1 = p.N1 / 3, K2 = p.N2 > 1 ? 2 * (p.N2 / 3) - 1 : 1;
   const int plane = (K1 * K2 + 15) / 16 * 16;
@@ -53,7 +57,9 @@ void store(const Vec& x, float* host, const Params& p) {
 
 // stats layout: [0] newton iterations, [1] Jacobian actions, [2] batched
 // integrations, [3] seconds, [4] seconds inside integrations, [5] final
-// relative residual, [6] converged, [7] number of residuals n, [8..8+n) residuals
+// relative residual, [6] converged, [7] number of residuals n, [8..8+n)
+// residuals, then per Newton step i < n-1 its relative GMRES residual and
+// its Jacobian actions
 void write_stats(const NKStats& s, double* out, int cap) {
   if (!out || cap < 8) return;
   out[0] = s.newton_iterations;
@@ -66,6 +72,11 @@ void write_stats(const NKStats& s, double* out, int cap) {
   const int n = std::min((int)s.residuals.size(), cap - 8);
   out[7] = n;
   for (int i = 0; i < n; i++) out[8 + i] = s.residuals[i];
+  const int ng = std::min((int)s.gmres_residuals.size(), (cap - 8 - n) / 2);
+  for (int i = 0; i < ng; i++) {
+    out[8 + n + 2 * i] = s.gmres_residuals[i];
+    out[8 + n + 2 * i + 1] = s.gmres_vectors[i];
+  }
 }
 
 // BasicNewtonKrylov with the constraints of PseudoArclength (phase, averages)
@@ -107,7 +118,9 @@ extern "C" {
 const char* sfh_last_error(void) { return g_host_err.c_str(); }
 
 // params: N1,N2,N3,L1,L2,L3,Re,Pr,Ri,dt,background; opts: max_newton, krylov,
-// target, gmres_tol, Delta, fd_eps, jacobian (0 tangent-linear, 1 finite differences)
+// target, gmres_tol, Delta, fd_eps, jacobian (0 tangent-linear, 1 finite
+// differences), block (directions per batched Jacobian action; 0: one, which
+// also allows multiple shooting, M > 1; >= 1 needs M = 1)
 int sfh_newton_fixed(const double* params, int M, double T, int constrain, const float* guess, const double* opts,
                      float* out, double* stats, int stats_cap) {
   try {
@@ -116,9 +129,16 @@ int sfh_newton_fixed(const double* params, int M, double T, int constrain, const
     Vec x(c);
     load(x, guess, p);
     x.EnforceBCs();
-    FixedPoint nk(options_from(opts), T, constrain != 0);
-    if (constrain) nk.EnforceConstraints(x);
-    NKStats s = nk.Run(x);
+    NKStats s;
+    if (block_from(opts) > 0) {
+      BlockFixedPoint nk(options_from(opts), block_from(opts), T, constrain != 0);
+      if (constrain) nk.EnforceConstraints(x);
+      s = nk.Run(x);
+    } else {
+      FixedPoint nk(options_from(opts), T, constrain != 0);
+      if (constrain) nk.EnforceConstraints(x);
+      s = nk.Run(x);
+    }
     store(x, out, p);
     write_stats(s, stats, stats_cap);
     return 0;
@@ -137,8 +157,14 @@ int sfh_periodic_orbit(const double* params, int M, double T0, const float* gues
     load(x, guess, p);
     x.EnforceBCs();
     x.p = T0;
-    PeriodicOrbit nk(options_from(opts), x);
-    NKStats s = nk.Run(x);
+    NKStats s;
+    if (block_from(opts) > 0) {
+      BlockPeriodicOrbit nk(options_from(opts), block_from(opts), x);
+      s = nk.Run(x);
+    } else {
+      PeriodicOrbit nk(options_from(opts), x);
+      s = nk.Run(x);
+    }
     store(x, out, p);
     if (T_out) *T_out = x.p;
     write_stats(s, stats, stats_cap);
@@ -166,9 +192,16 @@ int sfh_arclength(const double* params, int M, double T, const float* x0, double
     load(X, guess, p);
     X.p = Ri_guess;
     X.EnforceBCs();
-    PseudoArclength nk(options_from(opts), X0, V, ds, T);
-    nk.EnforceConstraints(X);
-    NKStats s = nk.Run(X);
+    NKStats s;
+    if (block_from(opts) > 0) {
+      BlockPseudoArclength nk(options_from(opts), block_from(opts), X0, V, ds, T);
+      nk.EnforceConstraints(X);
+      s = nk.Run(X);
+    } else {
+      PseudoArclength nk(options_from(opts), X0, V, ds, T);
+      nk.EnforceConstraints(X);
+      s = nk.Run(X);
+    }
     store(X, out, p);
     if (Ri_out) *Ri_out = X.p;
     write_stats(s, stats, stats_cap);

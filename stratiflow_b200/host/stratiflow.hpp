@@ -11,7 +11,10 @@
 // Jacobian action of GMRES costs one batched integration over T/M.
 #pragma once
 
+#include <algorithm>
 #include <chrono>
+#include <cstdio>
+#include <cstdlib>
 #include <cmath>
 #include <functional>
 #include <memory>
@@ -22,6 +25,16 @@
 #include "stratiflow_b200.h"
 
 namespace stratiflow {
+
+// STRATIFLOW_VERBOSE=1 prints the Krylov and Newton progress to stderr, as
+// the reference prints its Newton steps (NewtonKrylov.h:47)
+inline bool verbose() {
+  static const bool v = [] {
+    const char* e = std::getenv("STRATIFLOW_VERBOSE");
+    return e && *e && *e != '0';
+  }();
+  return v;
+}
 
 inline void check(int rc) {
   if (rc != SF_OK) throw std::runtime_error(std::string("stratiflow_b200: ") + sf_last_error());
@@ -138,6 +151,15 @@ struct Context {
       check(sf_set_tangent(tangent->h(), M));
     }
     return *tangent;
+  }
+  // one base and s tangent-linear runs (block Krylov methods, M = 1)
+  std::unique_ptr<Solver> block_tangent;
+  Solver& block_tangent_solver(int s) {
+    if (!block_tangent || block_tangent->nrun() != s + 1) {
+      block_tangent.reset(new Solver(p, s + 1));
+      check(sf_set_tangent(block_tangent->h(), 1));
+    }
+    return *block_tangent;
   }
 };
 
@@ -274,6 +296,68 @@ inline void EvolveTangent(const Vec& x, const Vec& dx, double tau, double Ri, Ve
   c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// ------------------------------------------ dense FP64 helpers ----------
+// min |b - A y| for A m x n (row-major, m >= n) by Householder QR; returns
+// |b - A y| and y (zero where R's diagonal vanishes)
+inline double lsq_householder(std::vector<double> A, int m, int n, std::vector<double> b, std::vector<double>& y) {
+  for (int k = 0; k < n; k++) {
+    double nrm = 0;
+    for (int i = k; i < m; i++) nrm += A[(size_t)i * n + k] * A[(size_t)i * n + k];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0) continue;
+    const double a0 = A[(size_t)k * n + k];
+    const double alpha = a0 > 0 ? -nrm : nrm;
+    std::vector<double> v(m - k);
+    for (int i = k; i < m; i++) v[i - k] = A[(size_t)i * n + k];
+    v[0] -= alpha;
+    double vn = 0;
+    for (double t : v) vn += t * t;
+    if (vn == 0) continue;
+    for (int j = k; j < n; j++) {
+      double d = 0;
+      for (int i = k; i < m; i++) d += v[i - k] * A[(size_t)i * n + j];
+      d = 2 * d / vn;
+      for (int i = k; i < m; i++) A[(size_t)i * n + j] -= d * v[i - k];
+    }
+    double d = 0;
+    for (int i = k; i < m; i++) d += v[i - k] * b[i];
+    d = 2 * d / vn;
+    for (int i = k; i < m; i++) b[i] -= d * v[i - k];
+  }
+  y.assign(n, 0.0);
+  double rmax = 0;
+  for (int k = 0; k < n; k++) rmax = std::max(rmax, std::fabs(A[(size_t)k * n + k]));
+  for (int k = n - 1; k >= 0; k--) {
+    double t = b[k];
+    for (int j = k + 1; j < n; j++) t -= A[(size_t)k * n + j] * y[j];
+    const double rk = A[(size_t)k * n + k];
+    y[k] = std::fabs(rk) > 1e-13 * rmax ? t / rk : 0.0;
+  }
+  double r = 0;
+  for (int i = n; i < m; i++) r += b[i] * b[i];
+  return std::sqrt(r);
+}
+
+// lower Cholesky factor of the k x k SPD matrix G (row-major); false if G is
+// not numerically positive definite
+inline bool cholesky(const std::vector<double>& G, int k, std::vector<double>& L) {
+  L.assign((size_t)k * k, 0.0);
+  double dmax = 0;
+  for (int i = 0; i < k; i++) dmax = std::max(dmax, G[(size_t)i * k + i]);
+  for (int j = 0; j < k; j++) {
+    double d = G[(size_t)j * k + j];
+    for (int t = 0; t < j; t++) d -= L[(size_t)j * k + t] * L[(size_t)j * k + t];
+    if (!(d > 1e-24 * dmax)) return false;
+    L[(size_t)j * k + j] = std::sqrt(d);
+    for (int i = j + 1; i < k; i++) {
+      double v = G[(size_t)i * k + j];
+      for (int t = 0; t < j; t++) v -= L[(size_t)i * k + t] * L[(size_t)j * k + t];
+      L[(size_t)i * k + j] = v / L[(size_t)j * k + j];
+    }
+  }
+  return true;
+}
+
 // ------------------------------------------------------------ FP64 SVD ----
 // one-sided Jacobi SVD of an m x n matrix (m >= n), row-major A:
 // A = U diag(S) V^T, U m x n, V n x n
@@ -340,6 +424,8 @@ struct NKStats {
   double residual = 0;
   bool converged = false;
   std::vector<double> residuals;
+  std::vector<double> gmres_residuals;   // relative GMRES residual of each Newton step
+  std::vector<int> gmres_vectors;        // Jacobian actions of each Newton step
 };
 
 // NewtonKrylov<VectorType> (NewtonKrylov.h:1-241) with FP64 Gram-Schmidt,
@@ -384,7 +470,10 @@ class NewtonKrylov {
       x0_ = &x;
       F0_ = F.get();
       AtIterate(x, *F);
-      st.krylov_vectors += GMRES(*F);
+      const int used = GMRES(*F);
+      st.krylov_vectors += used;
+      st.gmres_vectors.push_back(used);
+      st.gmres_residuals.push_back(n_ > 0 ? ResidualQR() : 1.0);
       bool accepted = false;
       for (int attempt = 0; attempt < 8 && !accepted; attempt++) {
         double zn = 0;
@@ -458,10 +547,21 @@ class NewtonKrylov {
       if (hn > 0) *basis_[k] *= 1.0 / hn;
       basis_[k]->EnforceBCs();
       n_ = k;
-      double zn;
-      if (LeastSquares(1e300, zn) < opt.gmres_tol || !(hn > 1e-14 * beta_)) break;
+      const double rq = ResidualQR();
+      if (verbose() && (k % 10 == 0)) std::fprintf(stderr, "GMRES: %d vectors, relative residual %.3e\n", k, rq);
+      if (rq < opt.gmres_tol || !(hn > 1e-14 * beta_)) break;
     }
     return used;
+  }
+
+  // relative residual of the unconstrained least-squares problem (Householder QR)
+  double ResidualQR() {
+    const int K = opt.krylov, m = n_ + 1, n = n_;
+    std::vector<double> A((size_t)m * n), b(m, 0.0), y;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) A[(size_t)i * n + j] = H_[(size_t)i * (K - 1) + j];
+    b[0] = beta_;
+    return lsq_householder(A, m, n, b, y) / beta_;
   }
 
   // min |beta e_0 - H y| with |y| <= Delta through the SVD of H (Chandler &
@@ -519,6 +619,343 @@ class NewtonKrylov {
   }
 
   std::vector<double> y_;
+};
+
+// ----------------------------------------------- block Krylov vectors ----
+// n device vectors of one state (M = 1) plus the scalar of each
+// (ExtendedStateVector::p, ExtendedStateVector.h:6-96)
+class Block {
+ public:
+  Block(Context& c, int n) : n_(n), p(n, 0.0) { check(sf_vecs_create(c.solver->h(), n, &v_)); }
+  ~Block() { sf_vecs_destroy(v_); }
+  Block(const Block&) = delete;
+  Block& operator=(const Block&) = delete;
+  sf_vecs* v() const { return v_; }
+  int n() const { return n_; }
+
+ private:
+  int n_;
+  sf_vecs* v_ = nullptr;
+
+ public:
+  std::vector<double> p;
+};
+
+// G[i][k] = Dot(A[a+i], B[b+k]) + p products (ExtendedStateVector::Dot)
+inline std::vector<double> block_gram(const Block& A, int a, int na, const Block& B, int b, int nb, double Ri) {
+  std::vector<double> G((size_t)na * nb);
+  check(sf_vecs_gram(A.v(), a, na, B.v(), b, nb, Ri, G.data()));
+  for (int i = 0; i < na; i++)
+    for (int k = 0; k < nb; k++) G[(size_t)i * nb + k] += A.p[a + i] * B.p[b + k];
+  return G;
+}
+
+// B[b+k] += alpha sum_i C[i][k] A[a+i] (scalars too)
+inline void block_update(Block& B, int b, int nb, double alpha, const Block& A, int a, int na,
+                         const std::vector<double>& C) {
+  check(sf_vecs_update(B.v(), b, nb, alpha, A.v(), a, na, C.data()));
+  for (int k = 0; k < nb; k++) {
+    double t = 0;
+    for (int i = 0; i < na; i++) t += C[(size_t)i * nb + k] * A.p[a + i];
+    B.p[b + k] += alpha * t;
+  }
+}
+
+// Evolve's derivative at x0 over tau applied to V[a..a+k) into W[b..b+k):
+// one batched integration of the base and k tangent-linear runs
+// (sf_set_tangent); the scalars of W are zeroed
+inline void EvolveTangentBlock(const Vec& x0, double tau, double Ri, int s, const Block& V, int a, int k, Block& W,
+                               int b) {
+  Context& c = x0.ctx();
+  auto t0 = std::chrono::steady_clock::now();
+  Solver& S = c.block_tangent_solver(s);
+  const int nsteps = std::max(1, (int)std::ceil(tau / c.p.dt - 1e-9));
+  S.set_dt(tau / nsteps);
+  for (int r = 0; r <= s; r++) S.set_ri(r, Ri);
+  Vec base(x0);
+  check(sf_vecs_zero_pressure(base.v(), 0, 1));
+  check(sf_vecs_to_run(base.v(), 0, S.h(), 0, 1));
+  check(sf_vecs_zero_pressure(V.v(), a, k));
+  check(sf_vecs_to_run(V.v(), a, S.h(), 1, k));
+  check(sf_prepare(S.h()));
+  check(sf_step(S.h(), nsteps));
+  check(sf_vecs_from_run(W.v(), b, S.h(), 1, k));
+  check(sf_vecs_zero_pressure(W.v(), b, k));
+  check(sf_vecs_enforce_bcs(W.v(), b, k));
+  check(sf_vecs_synchronize(W.v()));
+  for (int i = 0; i < k; i++) W.p[b + i] = 0.0;
+  c.evolutions += 1;
+  c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Newton-Krylov (NewtonKrylov.h:1-241) for single-shooting problems with a
+// block Krylov solver: the residual is split into s pieces (fields x bands
+// of j1), so the block Krylov space contains GMRES's Krylov space of the
+// residual, and every Arnoldi step applies the Jacobian to s directions in
+// one batched tangent-linear integration. Gram-Schmidt is classical, twice
+// (CGS2), against the whole basis in FP64 on the device; each new block is
+// orthonormalised by Cholesky QR, twice. The least-squares residual is
+// checked after each block (Householder QR); the hookstep (trust region of
+// NewtonKrylov.h:179-216) uses the SVD of the final block Hessenberg matrix.
+class BlockNewtonKrylov {
+ public:
+  BlockNewtonKrylov(const NKOptions& o, int s) : opt(o), s_(std::max(1, std::min(s, 32))) {}
+  virtual ~BlockNewtonKrylov() = default;
+  NKOptions opt;
+
+  virtual Vec EvalFunction(const Vec& at) = 0;
+  virtual void EnforceConstraints(Vec& at) { (void)at; }
+  virtual void AtIterate(const Vec& x, const Vec& F) { (void)x; (void)F; }
+  // W[b..b+k) = J V[a..a+k) about x0 (including the scalar rows/columns)
+  virtual void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) = 0;
+
+  NKStats Run(Vec& x) {
+    NKStats st;
+    auto t0 = std::chrono::steady_clock::now();
+    Context& c = x.ctx();
+    if (c.M != 1) throw std::runtime_error("the block Newton-Krylov solver needs one segment (M = 1)");
+    const long long ev0 = c.evolutions;
+    const double es0 = c.evolve_seconds;
+    std::unique_ptr<Vec> F(new Vec(EvalFunction(x)));
+    double xn = std::max(x.Norm(), 1e-300);
+    double res = F->Norm() / xn;
+    double Delta = opt.Delta * xn;
+    st.residuals.push_back(res);
+    for (int it = 0; it < opt.max_newton && res >= opt.target; it++) {
+      x0_ = &x;
+      AtIterate(x, *F);
+      Vec rhs(*F);
+      rhs *= -1.0;
+      double gres = 1.0;
+      const int used = GMRES(x, rhs, gres);
+      st.krylov_vectors += used;
+      st.gmres_vectors.push_back(used);
+      st.gmres_residuals.push_back(gres);
+      bool accepted = false;
+      for (int attempt = 0; attempt < 8 && !accepted; attempt++) {
+        double zn = 0;
+        Vec dx = Hookstep(x, Delta, zn);
+        Vec xt(x);
+        xt.MulAdd(1.0, dx);
+        EnforceConstraints(xt);
+        EnforceConstraints(xt);
+        EnforceConstraints(xt);
+        std::unique_ptr<Vec> Ft(new Vec(EvalFunction(xt)));
+        const double rt = Ft->Norm() / std::max(xt.Norm(), 1e-300);
+        if (rt < res) {
+          x = xt;
+          F = std::move(Ft);
+          if (zn >= 0.9 * Delta && rt < 0.5 * res) Delta *= 2;
+          res = rt;
+          accepted = true;
+        } else {
+          Delta = 0.5 * std::min(Delta, zn);
+        }
+      }
+      st.newton_iterations++;
+      st.residuals.push_back(res);
+      if (verbose())
+        std::fprintf(stderr, "NEWTON STEP %d: relative residual %.3e (GMRES %.3e, %d vectors)%s\n", it + 1, res,
+                     gres, used, accepted ? "" : ", no step accepted");
+      if (!accepted) break;
+    }
+    st.residual = res;
+    st.converged = res < opt.target;
+    st.evolutions = c.evolutions - ev0;
+    st.evolve_seconds = c.evolve_seconds - es0;
+    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    x0_ = nullptr;
+    return st;
+  }
+
+ protected:
+  const Vec* x0_ = nullptr;
+  int s_;
+  int bw_ = 0;                       // block width in use
+  int n_ = 0;                        // basis vectors in the least-squares problem
+  std::unique_ptr<Block> V_, W_;
+  std::vector<double> H_;            // (cap + bw) x cap, row-major with stride cap
+  std::vector<double> b0_;           // right-hand side in the basis
+  int cap_ = 0;
+
+  // rhs = sum of its pieces: u1, (u2,) u3, b, each split into bands of j1
+  int Split(const Vec& rhs) {
+    const Params& P = rhs.ctx().p;
+    const int K1 = P.N1 / 3;
+    std::vector<int> fields = P.N2 > 1 ? std::vector<int>{0, 1, 2, 3} : std::vector<int>{0, 2, 3};
+    const int nbands = std::max(1, s_ / (int)fields.size());
+    std::vector<int> edges{0};
+    for (int q = 1; q < nbands; q++) edges.push_back(std::min(K1, 1 << (q - 1)));
+    edges.push_back(K1);
+    int n = 0;
+    const double rn2 = rhs.Dot(rhs);
+    for (int f : fields)
+      for (int q = 0; q < nbands; q++) {
+        if (edges[q] >= edges[q + 1]) continue;
+        check(sf_vecs_copy(V_->v(), n, rhs.v(), 0));
+        check(sf_vecs_band(V_->v(), n, 1 << f, edges[q], edges[q + 1]));
+        V_->p[n] = 0.0;
+        double d = 0;
+        check(sf_vecs_dot_sum(V_->v(), n, V_->v(), n, 1, rhs.ctx().p.Ri, &d));
+        if (d > 1e-20 * rn2) n++;   // pieces with no share of the residual are left out
+      }
+    if (rhs.p != 0.0 || n == 0) {   // the scalar row is a piece of its own
+      check(sf_vecs_scale(V_->v(), n, 0.0, 1));
+      V_->p[n] = rhs.p;
+      n++;
+    }
+    return n;
+  }
+
+  // dst[b..b+k) = src[a..a+k) L^-T with G = L L^T the Gram matrix of the
+  // source; returns false if it is rank deficient. R = L^T.
+  bool CholQR(const Block& src, int a, Block& dst, int b, int k, double Ri, std::vector<double>& R) {
+    std::vector<double> G = block_gram(src, a, k, src, a, k, Ri), L;
+    if (!cholesky(G, k, L)) return false;
+    // Linv^T: solve L^T X = I column by column -> C[i][j] = (L^-T)[i][j]
+    std::vector<double> C((size_t)k * k, 0.0);
+    for (int j = 0; j < k; j++) {   // column j of L^-T: solve L^T c = e_j
+      for (int i = k - 1; i >= 0; i--) {
+        double t = (i == j) ? 1.0 : 0.0;
+        for (int m = i + 1; m < k; m++) t -= L[(size_t)m * k + i] * C[(size_t)m * k + j];
+        C[(size_t)i * k + j] = t / L[(size_t)i * k + i];
+      }
+    }
+    check(sf_vecs_scale(dst.v(), b, 0.0, k));
+    for (int i = 0; i < k; i++) dst.p[b + i] = 0.0;
+    block_update(dst, b, k, 1.0, src, a, k, C);
+    R.assign((size_t)k * k, 0.0);
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++) R[(size_t)i * k + j] = L[(size_t)j * k + i];
+    return true;
+  }
+
+  // two passes of CholQR from W[0..k) into V[at..at+k), R = R2 R1
+  bool CholQR2(int at, int k, double Ri, std::vector<double>& R) {
+    std::vector<double> R1, R2;
+    if (!CholQR(*W_, 0, *V_, at, k, Ri, R1)) return false;
+    if (!CholQR(*V_, at, *W_, 0, k, Ri, R2)) return false;
+    for (int i = 0; i < k; i++) {
+      check(sf_vecs_copy(V_->v(), at + i, W_->v(), i));
+      V_->p[at + i] = W_->p[i];
+    }
+    R.assign((size_t)k * k, 0.0);
+    for (int i = 0; i < k; i++)
+      for (int j = 0; j < k; j++) {
+        double t = 0;
+        for (int m = 0; m < k; m++) t += R2[(size_t)i * k + m] * R1[(size_t)m * k + j];
+        R[(size_t)i * k + j] = t;
+      }
+    return true;
+  }
+
+  // least squares min |b0 - H y| over the first n columns
+  double Residual(int n, std::vector<double>& y) {
+    const int m = n + bw_;
+    std::vector<double> A((size_t)m * n), b(b0_.begin(), b0_.begin() + m);
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) A[(size_t)i * n + j] = H_[(size_t)i * cap_ + j];
+    return lsq_householder(A, m, n, b, y);
+  }
+
+  // block Arnoldi for J y = rhs; returns the Jacobian actions
+  int GMRES(const Vec& x0, const Vec& rhs, double& rel) {
+    Context& c = rhs.ctx();
+    const double Ri = c.p.Ri;
+    cap_ = std::max(opt.krylov / s_, 1) * s_;
+    if (!V_ || V_->n() < cap_ + s_ + 1) V_.reset(new Block(c, cap_ + s_ + 1));
+    if (!W_ || W_->n() < s_ + 1) W_.reset(new Block(c, s_ + 1));
+    // the pieces of the residual, orthonormalised: rhs = V_1 R_1 (1,..,1)
+    int k = Split(rhs);
+    for (int i = 0; i < k; i++) {
+      check(sf_vecs_copy(W_->v(), i, V_->v(), i));
+      W_->p[i] = V_->p[i];
+    }
+    std::vector<double> R;
+    while (k > 0 && !CholQR2(0, k, Ri, R)) k--;   // drop trailing pieces until independent
+    bw_ = k;
+    H_.assign((size_t)(cap_ + bw_) * cap_, 0.0);
+    b0_.assign(cap_ + bw_, 0.0);
+    for (int i = 0; i < bw_; i++)
+      for (int j = 0; j < bw_; j++) b0_[i] += R[(size_t)i * bw_ + j];
+    double bn = 0;
+    for (double t : b0_) bn += t * t;
+    bn = std::sqrt(bn);
+    n_ = 0;
+    rel = 1.0;
+    if (!(bn > 0) || bw_ == 0) return 0;
+    int used = 0;
+    std::vector<double> y;
+    for (int j = 0; (j + 1) * bw_ <= cap_; j++) {
+      const int nb = (j + 1) * bw_;   // basis vectors so far
+      ApplyJ(x0, *V_, j * bw_, bw_, *W_, 0);
+      used += bw_;
+      for (int pass = 0; pass < 2; pass++) {
+        std::vector<double> C = block_gram(*V_, 0, nb, *W_, 0, bw_, Ri);
+        for (int i = 0; i < nb; i++)
+          for (int q = 0; q < bw_; q++) H_[(size_t)i * cap_ + j * bw_ + q] += C[(size_t)i * bw_ + q];
+        block_update(*W_, 0, bw_, -1.0, *V_, 0, nb, C);
+      }
+      std::vector<double> Rn;
+      const bool ok = nb + bw_ <= cap_ + bw_ && CholQR2(nb, bw_, Ri, Rn);
+      if (ok)
+        for (int i = 0; i < bw_; i++)
+          for (int q = 0; q < bw_; q++) H_[(size_t)(nb + i) * cap_ + j * bw_ + q] = Rn[(size_t)i * bw_ + q];
+      n_ = nb;
+      rel = Residual(n_, y) / bn;
+      if (verbose())
+        std::fprintf(stderr, "block GMRES: %d vectors, relative residual %.3e%s\n", nb, rel,
+                     ok ? "" : " (new block rank deficient)");
+      if (!ok || rel < opt.gmres_tol) break;
+    }
+    return used;
+  }
+
+  // the trust-region step (NewtonKrylov.h:179-216) in the block basis
+  Vec Hookstep(const Vec& like, double Delta, double& znorm) {
+    Vec dx(like);
+    dx.Zero();
+    znorm = 0;
+    if (n_ == 0) return dx;
+    const int m = n_ + bw_, n = n_;
+    std::vector<double> sub((size_t)m * n), U, S, Vv;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < n; j++) sub[(size_t)i * n + j] = H_[(size_t)i * cap_ + j];
+    svd(sub, m, n, U, S, Vv);
+    std::vector<double> pv(n, 0.0), z(n);
+    for (int j = 0; j < n; j++)
+      for (int i = 0; i < m; i++) pv[j] += U[(size_t)i * n + j] * b0_[i];
+    const double smax = *std::max_element(S.begin(), S.end());
+    auto zfor = [&](double mu) {
+      double t = 0;
+      for (int j = 0; j < n; j++) {
+        const double d = S[j];
+        z[j] = (d > 1e-13 * smax) ? pv[j] * d / (d * d + mu) : 0.0;
+        t += z[j] * z[j];
+      }
+      return std::sqrt(t);
+    };
+    double mu = 0;
+    if (zfor(0) > Delta) {
+      double lo = 0, hi = 1e-12;
+      while (zfor(hi) > Delta) hi *= 4;
+      for (int it = 0; it < 80; it++) {
+        const double mid = 0.5 * (lo + hi);
+        (zfor(mid) > Delta ? lo : hi) = mid;
+      }
+      mu = hi;
+    }
+    znorm = zfor(mu);
+    std::vector<double> y(n, 0.0);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < n; j++) y[i] += Vv[(size_t)i * n + j] * z[j];
+    check(sf_vecs_update(dx.v(), 0, 1, 1.0, V_->v(), 0, n, y.data()));
+    double p = 0;
+    for (int i = 0; i < n; i++) p += y[i] * V_->p[i];
+    dx.p = p;
+    dx.EnforceBCs();
+    return dx;
+  }
 };
 
 // F_i = Phi(x_i) - x_{i+1 mod M} for every segment i
@@ -640,6 +1077,137 @@ class PseudoArclength : public NewtonKrylov {
     r.MulAdd(dir.p, *dphi_dri_);
     r.p = -v_.Dot(dir);
     return r;
+  }
+
+ private:
+  Vec x0c_, v_;
+  double ds_, T_;
+  std::unique_ptr<Vec> last_phi_, dphi_dri_;
+};
+
+// ------------------------------------------ block single-shooting problems
+// W_i -= V_i for i < k (the "- x" of F = Phi(x) - x)
+inline void subtract_identity(const Block& V, int a, int k, Block& W, int b) {
+  std::vector<double> I((size_t)k * k, 0.0);
+  for (int i = 0; i < k; i++) I[(size_t)i * k + i] = 1.0;
+  block_update(W, b, k, -1.0, V, a, k, I);
+}
+
+// BasicNewtonKrylov (BasicNewtonKrylov.h:5-14) for Phi_T(x) = x, with the
+// phase and average constraints of PseudoArclength.h:15-20
+class BlockFixedPoint : public BlockNewtonKrylov {
+ public:
+  BlockFixedPoint(const NKOptions& o, int s, double T, bool constrain)
+      : BlockNewtonKrylov(o, s), T_(T), constrain_(constrain) {}
+  Vec EvalFunction(const Vec& at) override {
+    Vec phi(at);
+    Evolve(at, T_, at.ctx().p.Ri, phi);
+    phi.MulAdd(-1.0, at);
+    phi.p = 0;
+    return phi;
+  }
+  void EnforceConstraints(Vec& at) override {
+    if (!constrain_) return;
+    at.RemovePhaseShift();
+    at.RemoveAverage(0);
+    at.RemoveAverage(3);
+  }
+  void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
+    EvolveTangentBlock(x0, T_, x0.ctx().p.Ri, k, V, a, k, W, b);
+    subtract_identity(V, a, k, W, b);
+  }
+
+ private:
+  double T_;
+  bool constrain_;
+};
+
+// FindPeriodic (FindPeriodic.cpp:4-28): unknowns (x, p = T); F = Phi_T(x) - x,
+// F_p = n . (x - x_ref) with n the flow direction at the initial guess
+class BlockPeriodicOrbit : public BlockNewtonKrylov {
+ public:
+  BlockPeriodicOrbit(const NKOptions& o, int s, const Vec& guess)
+      : BlockNewtonKrylov(o, s), ref_(guess), normal_(guess) {
+    Context& c = guess.ctx();
+    Vec e1(guess), e2(guess);
+    Evolve(guess, c.p.dt, c.p.Ri, e1, &e2);
+    normal_ = e2;
+    normal_.MulAdd(-1.0, e1);
+    normal_ *= 1.0 / c.p.dt;
+    normal_.p = 0;
+  }
+  Vec EvalFunction(const Vec& at) override {
+    Context& c = at.ctx();
+    Vec phi(at), ext(at);
+    Evolve(at, at.p, c.p.Ri, phi, &ext);
+    ext.MulAdd(-1.0, phi);
+    ext *= 1.0 / c.solver->dt();
+    ext.p = 0;
+    last_f_.reset(new Vec(ext));
+    Vec d(at);
+    d.MulAdd(-1.0, ref_);
+    phi.MulAdd(-1.0, at);
+    phi.p = SegmentDot(normal_, d, 0);
+    return phi;
+  }
+  void AtIterate(const Vec& x, const Vec& F) override {
+    (void)x; (void)F;
+    f0_ = std::move(last_f_);
+  }
+  void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
+    Context& c = x0.ctx();
+    EvolveTangentBlock(x0, x0.p, c.p.Ri, k, V, a, k, W, b);
+    subtract_identity(V, a, k, W, b);
+    if (f0_) check(sf_vecs_update(W.v(), b, k, 1.0, f0_->v(), 0, 1, &V.p[a]));
+    std::vector<double> nd(k);
+    check(sf_vecs_gram(V.v(), a, k, normal_.v(), 0, 1, c.p.Ri, nd.data()));
+    for (int i = 0; i < k; i++) W.p[b + i] = nd[i];
+  }
+
+ private:
+  Vec ref_, normal_;
+  std::unique_ptr<Vec> last_f_, f0_;
+};
+
+// PseudoArclengthContinuation (PseudoArclength.h:6-42): unknowns (x, p = Ri)
+class BlockPseudoArclength : public BlockNewtonKrylov {
+ public:
+  BlockPseudoArclength(const NKOptions& o, int s, const Vec& x0, const Vec& v, double ds, double T)
+      : BlockNewtonKrylov(o, s), x0c_(x0), v_(v), ds_(ds), T_(T) {}
+  Vec EvalFunction(const Vec& at) override {
+    Vec phi(at);
+    Evolve(at, T_, at.p, phi);
+    last_phi_.reset(new Vec(phi));
+    phi.MulAdd(-1.0, at);
+    Vec d(at);
+    d.MulAdd(-1.0, x0c_);
+    phi.p = ds_ - v_.Dot(d);
+    return phi;
+  }
+  void EnforceConstraints(Vec& at) override {
+    at.RemovePhaseShift();
+    at.RemoveAverage(0);
+    at.RemoveAverage(3);
+  }
+  // dPhi/dRi at the Newton iterate by a one-sided difference in Ri
+  void AtIterate(const Vec& x, const Vec& F) override {
+    (void)F;
+    const double e = std::max(1e-3 * std::fabs(x.p), 1e-5);
+    Vec phi(x);
+    Evolve(x, T_, x.p + e, phi);
+    phi.MulAdd(-1.0, *last_phi_);
+    phi *= 1.0 / e;
+    phi.p = 0;
+    dphi_dri_.reset(new Vec(phi));
+  }
+  void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
+    Context& c = x0.ctx();
+    EvolveTangentBlock(x0, T_, x0.p, k, V, a, k, W, b);
+    subtract_identity(V, a, k, W, b);
+    check(sf_vecs_update(W.v(), b, k, 1.0, dphi_dri_->v(), 0, 1, &V.p[a]));
+    std::vector<double> vd(k);
+    check(sf_vecs_gram(V.v(), a, k, v_.v(), 0, 1, c.p.Ri, vd.data()));
+    for (int i = 0; i < k; i++) W.p[b + i] = -(vd[i] + v_.p * V.p[a + i]);
   }
 
  private:

@@ -3,8 +3,10 @@ of StateVector.h:40-149) and of the host drivers' Jacobian actions.
 
 Bounds: copies are exact; axpy / lincomb / scale agree with numpy on the same
 FP32 inputs to 1e-6 relative (one FP32 rounding per element); the FP64 dot
-products agree with the FP64 oracle energies and with a numpy FP64 restatement
-of StateVector::Dot to 1e-9 relative.
+products agree with the FP64 oracle energies and with a numpy FP64
+restatement of StateVector::Dot to 1e-7 of |x|^2: the device sums FP64
+products but holds the vertical quadrature weights in FP32, as the
+reference's FP32 build does.
 """
 import numpy as np
 import pytest
@@ -68,14 +70,15 @@ def test_vecs_dots_match_fp64(name):
     o = make_oracle(cfg, 64)
     o.set_state(s.get_state(0))
     ke, pe = o.energy()
-    assert abs(dd[0] - 2 * (ke + pe)) <= 1e-9 * abs(dd[0])   # StateVector::Dot = 2 (KE + PE)
+    # StateVector::Dot = 2 (KE + PE); the oracle sums its quadrature in another order
+    assert abs(dd[0] - 2 * (ke + pe)) <= 1e-7 * abs(dd[0])
     flow = _flow(cfg)
     a, b = V.get(0), V.get(1)
     ref01 = D.ext_dot(flow, (a, 0.0), (b, 0.0), Ri)
-    assert abs(dd[1] - ref01) <= 1e-9 * abs(dd[0])
+    assert abs(dd[1] - ref01) <= 1e-7 * abs(dd[0])
     tot = V.dot_sum(0, V, 0, 2, Ri)
     ref = D.ext_dot(flow, (a, 0.0), (a, 0.0), Ri) + D.ext_dot(flow, (b, 0.0), (b, 0.0), Ri)
-    assert abs(tot - ref) <= 1e-9 * abs(ref)
+    assert abs(tot - ref) <= 1e-7 * abs(ref)
 
 
 def test_phase_shift_and_average_match_reference_formulas():
@@ -110,17 +113,30 @@ def test_phase_shift_and_average_match_reference_formulas():
         assert np.allclose(after, col - integ / cfg_L3 / 2, rtol=0, atol=1e-6 * max(1e-30, np.abs(col).max()))
 
 
-def test_enforce_bcs_is_idempotent_on_solver_states():
+def _enforce_bcs(a):
+    """StateVector::EnforceBCs (StateVector.h:415-421) in numpy."""
+    a = a.copy()
+    N3 = a.shape[1]
+    a[2, [0, 1, 2, N3 - 2, N3 - 1]] = 0
+    for f in (0, 1, 3):
+        a[f, 0] = a[f, 1]
+        a[f, N3 - 1] = a[f, N3 - 2]
+    return a
+
+
+def test_enforce_bcs_matches_reference_formula():
+    """StateVector::EnforceBCs (StateVector.h:415-421): u3 ZeroEnds (levels
+    0, 1, 2, N3-2, N3-1 of a Dirichlet field, Field.h:475-486), u1, u2, b
+    NeumannEnds (level 0 = level 1, N3-1 = N3-2, Field.h:488-500)."""
     import stratiflow_b200 as sf
     cfg, s = _solver_with_states("shear3d_small", 1)
     V = sf.Vecs(s, 1)
     V.from_run(0, 0)
     a = V.get(0)
     V.enforce_bcs(0)
-    b = V.get(0)
-    V.enforce_bcs(0)
-    assert np.array_equal(V.get(0), b)
-    assert rel_l2(b, a) < 1e-6
+    want = _enforce_bcs(a)
+    want[:, :, s.K1 * s.K2:] = a[:, :, s.K1 * s.K2:]
+    assert np.array_equal(V.get(0), want)
 
 
 def test_driver_tangent_matches_central_difference():
@@ -145,3 +161,62 @@ def test_driver_tangent_matches_central_difference():
     fm = D.evolve(flow, X - eps * Dd, tau, M=2)
     fd = (fp.astype(np.complex128) - fm) / (2 * eps)
     assert rel_l2(j[:, :4], fd[:, :4]) < 1e-3
+
+
+def test_block_gram_update_and_band():
+    """sf_vecs_gram / sf_vecs_update / sf_vecs_band against numpy and the
+    one-pair dot product."""
+    import stratiflow_b200 as sf
+    cfg, s = _solver_with_states("kh2d", 3)
+    V = sf.Vecs(s, 6)
+    V.from_run(0, 0, 3)
+    V.from_run(3, 0, 3)
+    V.scale(3, -0.5, 3)
+    Ri = cfg["Ri"]
+    G = V.gram(0, 3, V, 3, 3, Ri)
+    for i in range(3):
+        for k in range(3):
+            d = V.dots(i, 1, V, 3 + k, Ri)[0]
+            assert abs(G[i, k] - d) <= 1e-12 * abs(V.dots(i, 1, V, i, Ri)[0])
+    a = [V.get(i) for i in range(6)]
+    C = np.array([[1.0, 0.5, -2.0], [0.25, -1.0, 3.0], [0.0, 2.0, 1.0]])
+    V.update(3, 3, 0.75, V, 0, 3, C)
+    for k in range(3):
+        want = a[3 + k].astype(np.complex128)
+        want[:4] += 0.75 * sum(C[i, k] * a[i][:4] for i in range(3))
+        assert rel_l2(V.get(3 + k), want) < 1e-6
+    V.band(0, 0b1001, 1, 4)   # u1 and b, 1 <= j1 < 4
+    got = V.get(0)
+    j1 = np.arange(s.plane) % s.K1
+    keep = (j1 >= 1) & (j1 < 4) & (np.arange(s.plane) < s.K1 * s.K2)
+    want = np.zeros_like(a[0])
+    for f in (0, 3):
+        want[f][:, keep] = a[0][f][:, keep]
+    assert np.array_equal(got, want)
+
+
+def test_block_newton_step_solves_the_linear_model():
+    """One block Newton-Krylov step of Phi_T(x) = x (T = 0.3, 16 directions
+    per batched Jacobian action, trust region wide open): the step dx it
+    takes leaves |J dx + F| / |F| equal to the block GMRES residual it
+    reports, with J dx = Phi'(x) dx - dx from the tangent-linear driver."""
+    from stratiflow_b200 import drivers as D
+    cfg = CONFIGS["kh2d"]
+    flow = _flow(cfg)
+    s = gpu_solver(cfg)
+    s.set_state(0, make_ic(cfg, seed=91, amp=5e-2))
+    s.Prepare()
+    x = _enforce_bcs(s.get_state_kept()[0])
+    x[4] = 0
+    T = 0.3
+    out, st = D.newton_fixed(flow, x, T, M=1, constrain=False,
+                             opts=D.NKOptions(max_newton=1, krylov=96, gmres_tol=1e-3, Delta=1e6, block=16))
+    assert st["newton_iterations"] == 1 and st["residuals"][1] < st["residuals"][0]
+    dx = out[0].astype(np.complex128) - x
+    dx[4] = 0
+    F = D.evolve(flow, x, T)[0].astype(np.complex128) - x
+    F[4] = 0
+    Jdx = D.evolve_tangent(flow, x, dx.astype(np.complex64), T)[0].astype(np.complex128) - dx
+    r = Jdx + F
+    rel = np.sqrt(D.ext_dot(flow, (r, 0.0), (r, 0.0), cfg["Ri"]) / D.ext_dot(flow, (F, 0.0), (F, 0.0), cfg["Ri"]))
+    assert abs(rel - st["gmres_residuals"][0]) < 0.02, (rel, st["gmres_residuals"][0])
