@@ -161,6 +161,19 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+def ncu_traffic(config, kernel):
+    """DRAM bytes (read + write) per launch of `kernel` on this workload from
+    one ncu capture, as recorded in profiles/dram_traffic.json (None if the
+    kernel has no capture there)."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            rec = json.load(f).get(config, {}).get(kernel)
+        return None if rec is None else float(rec["bytes_per_launch"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
 def kernel_bytes(s, name):
     """Compulsory HBM bytes of one launch of a kernel in this decomposition:
     S = one kept-mode complex64 field (N3*K1*K2*8 B per run), M = one
@@ -383,6 +396,7 @@ def main():
     dom_ms = per_kernel[dom][0] / per_kernel[dom][1]
     hbm, bf16, src = peaks()
     achieved = kernel_bytes(s, dom) / (dom_ms / 1e3) / 1e9
+    traffic = ncu_traffic(args.config, dom)
     step_bytes = step_bytes_model(s)
     step_ach = step_bytes * (value / ws) / 1e9
 
@@ -397,7 +411,7 @@ def main():
         "config": workload_config(args, wl),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_source": src + " (MEASURED_PEAKS.json hbm_gbs)"
-                     if src == "measured" else src, "traffic": None,
+                     if src == "measured" else src, "traffic": traffic,
                      "algorithmic_bytes_per_launch": kernel_bytes(s, dom), "launch_ms": dom_ms},
         "step_roofline": {"bytes_per_step": step_bytes, "achieved": step_ach, "peak": hbm, "unit": "GB/s",
                           "frac": step_ach / hbm},

@@ -216,6 +216,9 @@ int sf_vecs_update(sf_vecs* w, int b, int nb, double alpha, sf_vecs* v, int a, i
 /* keep only the fields of field_mask (bit 0 u1, 1 u2, 2 u3, 3 b) and the
  * modes with j1_lo <= j1 < j1_hi in vector i; p is zeroed */
 int sf_vecs_band(sf_vecs* v, int i, int field_mask, int j1_lo, int j1_hi);
+/* the z column (N3 complex values) of kept mode `mode` of `field` of vector
+ * i, to the host (write = 0) or from it (write = 1); synchronises */
+int sf_vecs_column(sf_vecs* v, int i, int field, int mode, float* host, int write);
 /* zero the p field of vectors i..i+count-1 */
 int sf_vecs_zero_pressure(sf_vecs* v, int i, int count);
 int sf_vecs_synchronize(sf_vecs* v);

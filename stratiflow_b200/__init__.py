@@ -36,7 +36,7 @@ EXPORTS = [
     "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
-    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band",
+    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column",
 ]
 
 
@@ -92,7 +92,7 @@ def load_library(path: str | None = None):
         "sf_net_set_params": [vp, fp], "sf_net_forward": [vp, fp, i, fp], "sf_net_set_data": [vp, fp, fp, i],
         "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
         "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
-        "sf_vecs_band": [vp, i, i, i, i],
+        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -366,6 +366,16 @@ class Vecs:
 
     def band(self, i, field_mask, j1_lo, j1_hi):
         _check(load_library().sf_vecs_band(self._h, int(i), int(field_mask), int(j1_lo), int(j1_hi)))
+
+    def column(self, i, field, mode):
+        out = np.zeros(self.solver.N3, dtype=np.complex64)
+        _check(load_library().sf_vecs_column(self._h, int(i), int(field), int(mode), _fptr(out), 0))
+        return out
+
+    def set_column(self, i, field, mode, col):
+        col = np.ascontiguousarray(col, dtype=np.complex64)
+        assert col.shape == (self.solver.N3,)
+        _check(load_library().sf_vecs_column(self._h, int(i), int(field), int(mode), _fptr(col), 1))
 
     def zero_pressure(self, i, count=1):
         _check(load_library().sf_vecs_zero_pressure(self._h, int(i), int(count)))

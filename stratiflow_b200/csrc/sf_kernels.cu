@@ -596,35 +596,37 @@ __global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
 // ------------------------------------------------ chunked z solves ----
 // The Thomas sweeps are first-order affine recurrences: D_j = al_j D_{j-1} +
 // be_j (al_j = -a_j/den_j, be_j = R_j/den_j) upward, x_j = D_j - C_j x_{j+1}
-// downward. A block of kZW warps splits N3 into kZW z-chunks, one per warp,
+// downward. A block of ZW warps (8, or 16 for grids too small to fill the
+// GPU) splits N3 into ZW z-chunks, one per warp,
 // and covers 16 modes x {real, imag} per warp: every chunk composes its
-// affine map, one warp scans the kZW maps in z order, and every chunk then
+// affine map, one warp scans the ZW maps in z order, and every chunk then
 // replays its levels from the right incoming value. be_j and D_j stay in
 // shared memory ([N3][32] floats per block). The result equals the sequential
 // sweep up to rounding.
-constexpr int kZW = 8;
 constexpr int kZU2 = 4;   // levels loaded ahead in the chunked z kernels
 
+template <int ZW>
 __device__ __forceinline__ void zscan_up(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
   sA[w * 32 + lane] = A;
   sB[w * 32 + lane] = B;
   __syncthreads();
   if (w == 0) {
     float v = 0.f;
-    for (int k = 0; k < kZW; k++) {
+    for (int k = 0; k < ZW; k++) {
       sIn[k * 32 + lane] = v;
       v = sA[k * 32 + lane] * v + sB[k * 32 + lane];
     }
   }
   __syncthreads();
 }
+template <int ZW>
 __device__ __forceinline__ void zscan_down(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
   sA[w * 32 + lane] = A;
   sB[w * 32 + lane] = B;
   __syncthreads();
   if (w == 0) {
     float v = 0.f;
-    for (int k = kZW - 1; k >= 0; k--) {
+    for (int k = ZW - 1; k >= 0; k--) {
       sIn[k * 32 + lane] = v;
       v = sA[k * 32 + lane] * v + sB[k * 32 + lane];
     }
@@ -632,9 +634,21 @@ __device__ __forceinline__ void zscan_down(float* sA, float* sB, float* sIn, int
   __syncthreads();
 }
 
+// the inverse pivots of levels j0, j0 + step, ... (kZU2 of them, those in
+// [lo, hi)) loaded ahead of their use in the serial sweeps
+__device__ __forceinline__ void load_iden(float (&bi)[kZU2], const float* __restrict__ iden, int Pp, int j0, int step,
+                                          int lo, int hi) {
+#pragma unroll
+  for (int i = 0; i < kZU2; i++) {
+    const int j = j0 + step * i;
+    bi[i] = (j >= lo && j < hi) ? iden[(size_t)j * Pp] : 0.f;
+  }
+}
+
 // k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
 // FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
-__global__ void __launch_bounds__(kZW * 32, 3) k_z_cn_chunked(StageArgs a) {
+template <int ZW>
+__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(StageArgs a) {
   const Geo g = a.g;
   extern __shared__ float zsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -645,12 +659,12 @@ __global__ void __launch_bounds__(kZW * 32, 3) k_z_cn_chunked(StageArgs a) {
   const int fi = blockIdx.y;
   const int f = g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
   const int N3 = g.N3, Pp = g.Pp;
-  const int chunk = (N3 + kZW - 1) / kZW;
+  const int chunk = (N3 + ZW - 1) / ZW;
   const int js = min(N3, w * chunk), je = min(N3, js + chunk);
   float* sD = zsm;                      // [N3][32]: be_j, then D_j
-  float* sA = zsm + (size_t)N3 * 32;    // [kZW][32]
-  float* sB = sA + kZW * 32;
-  float* sIn = sB + kZW * 32;
+  float* sA = zsm + (size_t)N3 * 32;    // [ZW][32]
+  float* sB = sA + ZW * 32;
+  float* sIn = sB + ZW * 32;
   const int q = m / g.K1, j1 = m - q * g.K1;
   const float kxv = a.kx[j1], kyv = a.ky[q];
   const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
@@ -751,30 +765,51 @@ __global__ void __launch_bounds__(kZW * 32, 3) k_z_cn_chunked(StageArgs a) {
       u0 = up;
     }
   }
-  zscan_up(sA, sB, sIn, w, lane, A, B);
+  zscan_up<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- forward, pass 2: D_j ----
   float D = sIn[w * 32 + lane];
-  for (int j = js; j < je; j++) {
-    const float al = (j == 0) ? 0.f : -fa[j] * iden[(size_t)j * Pp];
-    D = al * D + sD[j * 32 + lane];
-    sD[j * 32 + lane] = D;
+  for (int j0 = js; j0 < je; j0 += kZU2) {
+    float bi[kZU2];
+    load_iden(bi, iden, Pp, j0, 1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 + i;
+      if (j >= je) break;
+      const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
+      D = al * D + sD[j * 32 + lane];
+      sD[j * 32 + lane] = D;
+    }
   }
   // ---- backward, pass 1: chunk map of x_j = D_j - C_j x_{j+1} ----
   A = 1.f;
   B = 0.f;
-  for (int j = je - 1; j >= js; j--) {
-    const float Cj = fc[j] * iden[(size_t)j * Pp];
-    A = -Cj * A;
-    B = -Cj * B + sD[j * 32 + lane];
+  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
+    float bi[kZU2];
+    load_iden(bi, iden, Pp, j0, -1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 - i;
+      if (j < js) break;
+      const float Cj = fc[j] * bi[i];
+      A = -Cj * A;
+      B = -Cj * B + sD[j * 32 + lane];
+    }
   }
   __syncthreads();
-  zscan_down(sA, sB, sIn, w, lane, A, B);
+  zscan_down<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- backward, pass 2: the solution ----
   float x = sIn[w * 32 + lane];
-  for (int j = je - 1; j >= js; j--) {
-    const float Cj = fc[j] * iden[(size_t)j * Pp];
-    x = sD[j * 32 + lane] - Cj * x;
-    if (act) out[j * S2] = x;
+  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
+    float bi[kZU2];
+    load_iden(bi, iden, Pp, j0, -1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 - i;
+      if (j < js) break;
+      const float Cj = fc[j] * bi[i];
+      x = sD[j * 32 + lane] - Cj * x;
+      if (act) out[j * S2] = x;
+    }
   }
 }
 
@@ -782,7 +817,8 @@ __global__ void __launch_bounds__(kZW * 32, 3) k_z_cn_chunked(StageArgs a) {
 // divergence and the Laplacian factors upward, q downward, then u -= grad q
 // and p += pm q. The two components of a mode are adjacent lanes and
 // exchange q; u3_{j+1} at a chunk's top uses the next chunk's q from the scan.
-__global__ void __launch_bounds__(kZW * 32, 3) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
+template <int ZW>
+__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
                                                            const float* zc, const float* fa, const float* fc,
                                                            const float* inv_den, const float* kx, const float* ky,
                                                            float pm) {
@@ -793,12 +829,12 @@ __global__ void __launch_bounds__(kZW * 32, 3) k_z_proj_chunked(Geo g, float2* U
   const int m = act ? m0 : 0;
   const int run = blockIdx.z;
   const int N3 = g.N3, Pp = g.Pp;
-  const int chunk = (N3 + kZW - 1) / kZW;
+  const int chunk = (N3 + ZW - 1) / ZW;
   const int js = min(N3, w * chunk), je = min(N3, js + chunk);
   float* sD = zsm;
   float* sA = zsm + (size_t)N3 * 32;
-  float* sB = sA + kZW * 32;
-  float* sIn = sB + kZW * 32;
+  float* sB = sA + ZW * 32;
+  float* sIn = sB + ZW * 32;
   const int q = m / g.K1, j1 = m - q * g.K1;
   const float kxv = kx[j1], kyv = g.dim3 ? ky[q] : 0.f;
   const float sc = c == 0 ? -1.f : 1.f;
@@ -849,41 +885,67 @@ __global__ void __launch_bounds__(kZW * 32, 3) k_z_proj_chunked(Geo g, float2* U
       w0 = w1;
     }
   }
-  zscan_up(sA, sB, sIn, w, lane, A, B);
+  zscan_up<ZW>(sA, sB, sIn, w, lane, A, B);
   float D = sIn[w * 32 + lane];
-  for (int j = js; j < je; j++) {
-    const float al = (j == 0) ? 0.f : -a_[j] * iden[(size_t)j * Pp];
-    D = al * D + sD[j * 32 + lane];
-    sD[j * 32 + lane] = D;
+  for (int j0 = js; j0 < je; j0 += kZU2) {
+    float bi[kZU2];
+    load_iden(bi, iden, Pp, j0, 1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 + i;
+      if (j >= je) break;
+      const float al = (j == 0) ? 0.f : -a_[j] * bi[i];
+      D = al * D + sD[j * 32 + lane];
+      sD[j * 32 + lane] = D;
+    }
   }
   // ---- backward: q ----
-  auto Cof = [&](int j) {
-    float Cj = c_[j] * iden[(size_t)j * Pp];
+  auto Cof = [&](int j, float bij) {
+    float Cj = c_[j] * bij;
     if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
     return Cj;
   };
   A = 1.f;
   B = 0.f;
-  for (int j = je - 1; j >= js; j--) {
-    const float Cj = Cof(j);
-    A = -Cj * A;
-    B = -Cj * B + sD[j * 32 + lane];
+  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
+    float bi[kZU2];
+    load_iden(bi, iden, Pp, j0, -1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 - i;
+      if (j < js) break;
+      const float Cj = Cof(j, bi[i]);
+      A = -Cj * A;
+      B = -Cj * B + sD[j * 32 + lane];
+    }
   }
   __syncthreads();
-  zscan_down(sA, sB, sIn, w, lane, A, B);
+  zscan_down<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- backward, pass 2: q_j, projection, p ----
   float qn = sIn[w * 32 + lane];   // q at level je (0 above the top)
-  for (int j = je - 1; j >= js; j--) {
-    const float qj = sD[j * 32 + lane] - Cof(j) * qn;
-    const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
-    if (act) {
-      u1c[j * S2] -= sc * kxv * qo;
-      if (g.dim3) u2c[j * S2] -= sc * kyv * qo;
-      pd[j * S2] = ps[j * S2] + pm * qj;
-      const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
-      if (jj >= 2 && jj <= N3 - 1) u3[jj * S2] -= dnd_lo[jj] * qj + dnd_di[jj] * qn;
+  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
+    float bi[kZU2], pv[kZU2];
+    load_iden(bi, iden, Pp, j0, -1, js, je);
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 - i;
+      pv[i] = (j >= js && act) ? ps[j * S2] : 0.f;
     }
-    qn = qj;
+#pragma unroll
+    for (int i = 0; i < kZU2; i++) {
+      const int j = j0 - i;
+      if (j < js) break;
+      const float qj = sD[j * 32 + lane] - Cof(j, bi[i]) * qn;
+      const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
+      if (act) {
+        u1c[j * S2] -= sc * kxv * qo;
+        if (g.dim3) u2c[j * S2] -= sc * kyv * qo;
+        pd[j * S2] = pv[i] + pm * qj;
+        const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
+        if (jj >= 2 && jj <= N3 - 1) u3[jj * S2] -= dnd_lo[jj] * qj + dnd_di[jj] * qn;
+      }
+      qn = qj;
+    }
   }
 }
 
@@ -1218,17 +1280,28 @@ int prepare_kernels() {
   ATTR((k_xpass<128, false>)) ATTR((k_xpass<256, false>)) ATTR((k_xpass<512, false>))
   ATTR((k_xpass<16, true>)) ATTR((k_xpass<32, true>)) ATTR((k_xpass<64, true>))
   ATTR((k_xpass<128, true>)) ATTR((k_xpass<256, true>)) ATTR((k_xpass<512, true>))
-  ATTR(k_z_cn_chunked) ATTR(k_z_proj_chunked)
+  ATTR(k_z_cn_chunked<8>) ATTR(k_z_proj_chunked<8>) ATTR(k_z_cn_chunked<16>) ATTR(k_z_proj_chunked<16>)
 #undef ATTR
   return e == cudaSuccess ? 0 : -1;
 }
 
-static size_t zchunk_smem(const Geo& g) { return sizeof(float) * ((size_t)g.N3 * 32 + 3 * kZW * 32); }
+static size_t zchunk_smem(const Geo& g, int zw) { return sizeof(float) * ((size_t)g.N3 * 32 + 3 * zw * 32); }
+
+// z chunks per block: 16 (shorter serial sweeps, one 16-warp block per SM)
+// when the grid leaves SMs without a block, else 8 (three blocks per SM)
+static int z_chunks(const Geo& g, int fields) {
+  return (long long)cdiv(g.P, 16) * fields * g.nrun < 148 ? 16 : 8;
+}
 
 int launch_project(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
-  k_z_proj_chunked<<<dim3(cdiv(g.P, 16), 1, g.nrun), kZW * 32, zchunk_smem(g), st>>>(
-      g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc, a.inv_den, a.kx, a.ky, a.pm);
+  const dim3 grid(cdiv(g.P, 16), 1, g.nrun);
+  if (z_chunks(g, 1) == 16)
+    k_z_proj_chunked<16><<<grid, 16 * 32, zchunk_smem(g, 16), st>>>(g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc,
+                                                                      a.inv_den, a.kx, a.ky, a.pm);
+  else
+    k_z_proj_chunked<8><<<grid, 8 * 32, zchunk_smem(g, 8), st>>>(g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc, a.inv_den,
+                                                                   a.kx, a.ky, a.pm);
   return 1;
 }
 
@@ -1250,17 +1323,22 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     launch_ifft_y(a, g.nrun, st);
     mark();
   }
-  n += launch_xpass(a, st) - 1;   // counts the kernels, the mark below adds one
+  const int extra = launch_xpass(a, st) - 1;   // a tangent-linear batch launches the x pass twice
   mark();
   if (g.dim3) {
     launch_fft_y(a, st);
     mark();
   }
-  k_z_cn_chunked<<<dim3(cdiv(g.P, 16), g.dim3 ? 4 : 3, g.nrun), kZW * 32, zchunk_smem(g), st>>>(a);
+  const int nf = g.dim3 ? 4 : 3;
+  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
+  if (z_chunks(g, nf) == 16)
+    k_z_cn_chunked<16><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+  else
+    k_z_cn_chunked<8><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
   mark();
   launch_project(a, st);
   mark();
-  return n;
+  return n + extra;
 }
 
 int launch_factor(const Geo& g, const double* bands, const double* kx, const double* ky, double h0, double h1,

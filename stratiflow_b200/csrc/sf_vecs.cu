@@ -513,6 +513,22 @@ int sf_vecs_band(sf_vecs* v, int i, int field_mask, int j1_lo, int j1_hi) {
   return SF_OK;
 }
 
+// copy the z column of one mode of one field of vector i (N3 complex values)
+// to the host (write = 0) or from it (write = 1)
+int sf_vecs_column(sf_vecs* v, int i, int field, int mode, float* host, int write) {
+  if (!v || !host || i < 0 || i >= v->nvec || field < 0 || field > 4 || mode < 0 || mode >= v->g.P)
+    return vfail(SF_EINVAL, "bad argument");
+  float2* col = v->d + (size_t)i * vstride(v->g) + (size_t)field * v->g.fblk + mode;
+  const size_t pitch = sizeof(float2) * v->g.Pp;
+  if (write) {
+    VCK(cudaMemcpy2DAsync(col, pitch, host, sizeof(float2), sizeof(float2), v->g.N3, cudaMemcpyHostToDevice, v->st));
+  } else {
+    VCK(cudaMemcpy2DAsync(host, sizeof(float2), col, pitch, sizeof(float2), v->g.N3, cudaMemcpyDeviceToHost, v->st));
+  }
+  VCK(cudaStreamSynchronize(v->st));
+  return SF_OK;
+}
+
 // zero the p field of vectors i..i+count-1
 int sf_vecs_zero_pressure(sf_vecs* v, int i, int count) {
   if (!v || count < 1 || i < 0 || i + count > v->nvec) return vfail(SF_EINVAL, "bad argument");

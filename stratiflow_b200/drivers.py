@@ -65,13 +65,17 @@ class NKOptions:
     "fd" (finite differences with step fd_eps |x|, NewtonKrylov.h:218-235).
     block: directions per batched Jacobian action of the block Krylov solver
     (single shooting, M = 1); 0 selects the one-direction solver, which also
-    runs multiple shooting. krylov: basis vectors before the solve stops."""
+    runs multiple shooting. krylov: basis vectors before the solve stops.
+    precondition: the block solvers' mean-flow preconditioner (the (0,0)
+    profiles of u1 and b relax by diffusion alone and are otherwise the
+    slowest directions for GMRES)."""
 
     def __init__(self, max_newton=20, krylov=80, target=1e-6, gmres_tol=0.01, Delta=100.0, fd_eps=3e-4,
-                 jacobian="tangent", block=16):
+                 jacobian="tangent", block=16, precondition=True):
         assert jacobian in ("tangent", "fd")
         self.v = np.array([max_newton, krylov, target, gmres_tol, Delta, fd_eps,
-                           0.0 if jacobian == "tangent" else 1.0, block], dtype=np.float64)
+                           0.0 if jacobian == "tangent" else 1.0, block, float(bool(precondition))],
+                          dtype=np.float64)
 
 
 def _opts(opts, M):
@@ -227,14 +231,15 @@ def secant_predictor(flow: Flow, p1, p2, ds):
 
 
 def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, predictor=None, log=None,
-                 fallback_after=6):
+                 fallback_after=6, stop_on_failure=False):
     """Pseudo-arclength continuation from two converged points
     ((x, Ri), (x, Ri)). `predictor(history, ds)` may replace the secant: it
     gets the converged points so far and returns a guess (x, Ri); the secant
     tangent is always used for the arclength constraint. A learned guess
     gets `fallback_after` Newton iterations; if it has not converged by then
-    the point is solved again from the secant guess. Returns the points and
-    the per-point statistics."""
+    the point is solved again from the secant guess. A point that does not
+    converge is kept at Newton's last iterate (and ends the run with
+    `stop_on_failure`). Returns the points and the per-point statistics."""
     pts = list(start_points)
     stats = []
     opts = opts or NKOptions()
@@ -265,7 +270,7 @@ def continuation(flow: Flow, start_points, ds, npoints, T=11.0, M=1, opts=None, 
         pts.append((x.reshape(flow.state_shape) if M == 1 else x, Ri))
         if log:
             log(k, st)
-        if not st["converged"]:
+        if not st["converged"] and stop_on_failure:
             break
     return pts, stats
 
@@ -321,10 +326,13 @@ class LearnedPredictor:
         out[:, 2 * self.nc + 1] = r2 / sri
         return out
 
-    def fit(self, points, ds, steps=1500, lr=1e-3):
+    def fit(self, points, ds, steps=600, lr=1e-3, holdout=2, chunk=50):
         """Train on consecutive triples of converged points (x, Ri): inputs
-        from the first two, target = third - secant guess. Returns the
-        losses."""
+        from the first two, target = third - secant guess. The last
+        `holdout` triples are held out: training keeps the parameters with
+        the lowest held-out loss, and if no parameters beat the secant guess
+        there (a zero correction) the predictor returns the secant guess.
+        Returns the training losses."""
         triples = [(points[k - 2], points[k - 1], points[k]) for k in range(2, len(points))]
         assert triples, "need at least three converged points"
         feats = [self._feat(p[0]) for p in points]
@@ -340,12 +348,34 @@ class LearnedPredictor:
         Y = np.zeros((len(triples), self.flow.N3, self.cout), dtype=np.float32)
         for i, t in enumerate(tg):
             Y[i, :, :self.nc] = t / self.scale["t"]
-        self.net.set_data(X, Y)
-        self.losses = self.net.train(steps, lr)
+        nh = holdout if len(triples) > holdout else 0
+        Xt, Yt = (X[:-nh], Y[:-nh]) if nh else (X, Y)
+        self.val_baseline = float(np.mean(Y[-nh:] ** 2)) if nh else None
+        best, best_loss, losses, self.val_losses = None, self.val_baseline, [], []
+        done = 0
+        while done < steps:
+            n = min(chunk, steps - done)
+            self.net.set_data(Xt, Yt)
+            losses.extend(self.net.train(n, lr))
+            done += n
+            if nh:
+                v = float(np.mean((self.net.forward(X[-nh:]) - Y[-nh:]) ** 2))
+                self.val_losses.append(v)
+                if v < best_loss:
+                    best, best_loss = self.net.get_params(), v
+        if nh:
+            self.use_net = best is not None
+            if best is not None:
+                self.net.set_params(best)
+        else:
+            self.use_net = True
+        self.losses = np.array(losses)
         return self.losses
 
     def __call__(self, pts, ds):
         sec_guess, _ = secant_predictor(self.flow, pts[-2], pts[-1], ds)
+        if not getattr(self, "use_net", True):
+            return sec_guess
         y = self.net.forward(self._inputs(pts[-2], pts[-1], ds)[None])[0]
         corr = self._unfeat(y[:, :self.nc].astype(np.float64) * self.scale["t"])
         return (sec_guess[0] + corr).astype(np.complex64), sec_guess[1]

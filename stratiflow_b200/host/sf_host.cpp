@@ -35,6 +35,7 @@ NKOptions options_from(const double* o) {
   n.Delta = o[4];
   n.fd_eps = o[5];
   n.tangent = o[6] == 0.0;   // 0: tangent-linear Jacobian actions, 1: finite differences
+  n.precondition = o[8] != 0.0;
   return n;
 }
 
@@ -120,7 +121,8 @@ const char* sfh_last_error(void) { return g_host_err.c_str(); }
 // params: N1,N2,N3,L1,L2,L3,Re,Pr,Ri,dt,background; opts: max_newton, krylov,
 // target, gmres_tol, Delta, fd_eps, jacobian (0 tangent-linear, 1 finite
 // differences), block (directions per batched Jacobian action; 0: one, which
-// also allows multiple shooting, M > 1; >= 1 needs M = 1)
+// also allows multiple shooting, M > 1; >= 1 needs M = 1), precondition (block
+// solvers: 1 applies the mean-flow preconditioner)
 int sfh_newton_fixed(const double* params, int M, double T, int constrain, const float* guess, const double* opts,
                      float* out, double* stats, int stats_cap) {
   try {

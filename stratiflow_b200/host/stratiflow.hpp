@@ -413,6 +413,7 @@ struct NKOptions {
   double fd_eps = 3e-4;       // finite-difference step relative to |x|
   bool tangent = true;        // Jacobian actions by the tangent-linear batch, else by
                               // finite differences (NewtonKrylov.h:218-235)
+  bool precondition = true;   // block solvers: the mean-flow preconditioner
 };
 
 struct NKStats {
@@ -688,6 +689,148 @@ inline void EvolveTangentBlock(const Vec& x0, double tau, double Ri, int s, cons
   c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// ------------------------------------------- mean-flow preconditioner ----
+// The slowest directions of F(x) = Phi_T(x) - x in a stratified shear layer
+// are the horizontally averaged profiles of u1 and b (the (0,0) modes): they
+// relax by vertical diffusion alone, over L3^2 Re ~ 1e5 time units, so
+// J = Phi_T' - I is nearly singular on them and GMRES needs many vectors to
+// resolve them. This right preconditioner applies M = (I - E + Pi)^-1 to the
+// (0,0) columns of u1 and b, with E = exp(T nu D2) the diffusion propagator
+// of the mean profile (D2 the Neumann second derivative of
+// Differentiation.cpp:6-33 with the ghost levels folded in, nu = 1/Re for u1
+// and 1/(Re Pr) for b) and Pi the projection on constant profiles (weights
+// DYF, which D2 conserves); everything else passes unchanged. Then J M is
+// close to -I on the mean profiles, as it is on the fast decaying modes.
+class MeanFlowPreconditioner {
+ public:
+  MeanFlowPreconditioner(const Params& p, double T) : N_(p.N3) {
+    const int N = p.N3, n = N - 2;
+    std::vector<double> z(N, 0.0), zf(N, 0.0), DY(N, 0.0), DYF(N, 0.0);
+    const double step = 2.0 / (N - 2);
+    for (int i = 0; i < N - 1; i++) {
+      const double x = (i == N - 2) ? 1.0 : -1.0 + i * step;
+      z[i + 1] = p.L3 * (2.0 * std::pow(x, 7) + x) / 3.0;
+    }
+    const double off = (z[1] + z[2]) / 2;
+    for (int i = 1; i < N; i++) z[i] *= -p.L3 / off;
+    for (int i = 1; i <= N - 2; i++) zf[i] = 0.5 * (z[i] + z[i + 1]);
+    zf[0] = 2 * zf[1] - zf[2];
+    zf[N - 1] = 2 * zf[N - 2] - zf[N - 3];
+    for (int i = 1; i < N; i++) DY[i] = zf[i] - zf[i - 1];
+    for (int i = 1; i <= N - 2; i++) DYF[i] = z[i + 1] - z[i];
+    // D2 on the interior levels 1..N-2, ghosts f_0 = f_1, f_{N-1} = f_{N-2}
+    std::vector<double> A((size_t)n * n, 0.0), w(n);
+    for (int j = 1; j <= N - 2; j++) {
+      const double lo = 1 / DY[j] / DYF[j], up = 1 / DY[j + 1] / DYF[j], r = j - 1;
+      A[(size_t)r * n + r] += -lo - up;
+      A[(size_t)r * n + (j == 1 ? r : r - 1)] += lo;
+      A[(size_t)r * n + (j == N - 2 ? r : r + 1)] += up;
+      w[r] = DYF[j];
+    }
+    const double nus[2] = {1.0 / p.Re, 1.0 / (p.Re * p.Pr)};
+    for (int k = 0; k < 2; k++) {
+      std::vector<double> E = expm(A, n, T * nus[k]);
+      double ws = 0;
+      for (double t : w) ws += t;
+      for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++) E[(size_t)i * n + j] = (i == j ? 1.0 : 0.0) - E[(size_t)i * n + j] + w[j] / ws;
+      Minv_[k] = inverse(E, n);
+    }
+  }
+
+  // M applied in place to vectors a..a+k of a block (u1 and b (0,0) columns)
+  void Apply(sf_vecs* v, int a, int k) const {
+    const int N = N_, n = N - 2;
+    std::vector<float> col(2 * (size_t)N);
+    std::vector<double> f(n), g(n);
+    for (int i = a; i < a + k; i++)
+      for (int q = 0; q < 2; q++) {
+        const int field = q == 0 ? 0 : 3;
+        check(sf_vecs_column(v, i, field, 0, col.data(), 0));
+        for (int r = 0; r < n; r++) f[r] = col[2 * (r + 1)];
+        const std::vector<double>& M = Minv_[q];
+        for (int r = 0; r < n; r++) {
+          double t = 0;
+          for (int c = 0; c < n; c++) t += M[(size_t)r * n + c] * f[c];
+          g[r] = t;
+        }
+        for (int r = 0; r < n; r++) col[2 * (r + 1)] = (float)g[r];
+        col[0] = col[2];
+        col[2 * (N - 1)] = col[2 * (N - 2)];
+        check(sf_vecs_column(v, i, field, 0, col.data(), 1));
+      }
+  }
+
+ private:
+  int N_;
+  std::vector<double> Minv_[2];
+
+  static std::vector<double> matmul(const std::vector<double>& X, const std::vector<double>& Y, int n) {
+    std::vector<double> Z((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++)
+      for (int k = 0; k < n; k++) {
+        const double x = X[(size_t)i * n + k];
+        if (x == 0.0) continue;
+        for (int j = 0; j < n; j++) Z[(size_t)i * n + j] += x * Y[(size_t)k * n + j];
+      }
+    return Z;
+  }
+  // exp(c A) by scaling and squaring of a degree-16 Taylor polynomial
+  static std::vector<double> expm(const std::vector<double>& A, int n, double c) {
+    double nrm = 0;
+    for (int j = 0; j < n; j++) {
+      double t = 0;
+      for (int i = 0; i < n; i++) t += std::fabs(A[(size_t)i * n + j]);
+      nrm = std::max(nrm, t);
+    }
+    nrm *= std::fabs(c);
+    int sq = 0;
+    while (nrm / std::ldexp(1.0, sq) > 0.25) sq++;
+    const double scale = c / std::ldexp(1.0, sq);
+    std::vector<double> X((size_t)n * n), E((size_t)n * n, 0.0), term((size_t)n * n, 0.0);
+    for (size_t i = 0; i < X.size(); i++) X[i] = A[i] * scale;
+    for (int i = 0; i < n; i++) E[(size_t)i * n + i] = term[(size_t)i * n + i] = 1.0;
+    for (int k = 1; k <= 16; k++) {
+      term = matmul(term, X, n);
+      for (size_t i = 0; i < term.size(); i++) term[i] /= k;
+      for (size_t i = 0; i < E.size(); i++) E[i] += term[i];
+    }
+    for (int i = 0; i < sq; i++) E = matmul(E, E, n);
+    return E;
+  }
+  // Gauss-Jordan with partial pivoting
+  static std::vector<double> inverse(std::vector<double> A, int n) {
+    std::vector<double> B((size_t)n * n, 0.0);
+    for (int i = 0; i < n; i++) B[(size_t)i * n + i] = 1.0;
+    for (int c = 0; c < n; c++) {
+      int piv = c;
+      for (int r = c + 1; r < n; r++)
+        if (std::fabs(A[(size_t)r * n + c]) > std::fabs(A[(size_t)piv * n + c])) piv = r;
+      if (A[(size_t)piv * n + c] == 0.0) throw std::runtime_error("mean-flow preconditioner: singular matrix");
+      if (piv != c)
+        for (int j = 0; j < n; j++) {
+          std::swap(A[(size_t)piv * n + j], A[(size_t)c * n + j]);
+          std::swap(B[(size_t)piv * n + j], B[(size_t)c * n + j]);
+        }
+      const double d = 1.0 / A[(size_t)c * n + c];
+      for (int j = 0; j < n; j++) {
+        A[(size_t)c * n + j] *= d;
+        B[(size_t)c * n + j] *= d;
+      }
+      for (int r = 0; r < n; r++) {
+        if (r == c) continue;
+        const double f = A[(size_t)r * n + c];
+        if (f == 0.0) continue;
+        for (int j = 0; j < n; j++) {
+          A[(size_t)r * n + j] -= f * A[(size_t)c * n + j];
+          B[(size_t)r * n + j] -= f * B[(size_t)c * n + j];
+        }
+      }
+    }
+    return B;
+  }
+};
+
 // Newton-Krylov (NewtonKrylov.h:1-241) for single-shooting problems with a
 // block Krylov solver: the residual is split into s pieces (fields x bands
 // of j1), so the block Krylov space contains GMRES's Krylov space of the
@@ -708,12 +851,16 @@ class BlockNewtonKrylov {
   virtual void AtIterate(const Vec& x, const Vec& F) { (void)x; (void)F; }
   // W[b..b+k) = J V[a..a+k) about x0 (including the scalar rows/columns)
   virtual void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) = 0;
+  // the time over which the mean-flow preconditioner relaxes (0: none)
+  virtual double PreconditionerTime() const { return 0.0; }
 
   NKStats Run(Vec& x) {
     NKStats st;
     auto t0 = std::chrono::steady_clock::now();
     Context& c = x.ctx();
     if (c.M != 1) throw std::runtime_error("the block Newton-Krylov solver needs one segment (M = 1)");
+    if (opt.precondition && PreconditionerTime() > 0 && !prec_)
+      prec_.reset(new MeanFlowPreconditioner(c.p, PreconditionerTime()));
     const long long ev0 = c.evolutions;
     const double es0 = c.evolve_seconds;
     std::unique_ptr<Vec> F(new Vec(EvalFunction(x)));
@@ -773,7 +920,8 @@ class BlockNewtonKrylov {
   int s_;
   int bw_ = 0;                       // block width in use
   int n_ = 0;                        // basis vectors in the least-squares problem
-  std::unique_ptr<Block> V_, W_;
+  std::unique_ptr<Block> V_, W_, Z_;
+  std::unique_ptr<MeanFlowPreconditioner> prec_;
   std::vector<double> H_;            // (cap + bw) x cap, row-major with stride cap
   std::vector<double> b0_;           // right-hand side in the basis
   int cap_ = 0;
@@ -865,6 +1013,7 @@ class BlockNewtonKrylov {
     cap_ = std::max(opt.krylov / s_, 1) * s_;
     if (!V_ || V_->n() < cap_ + s_ + 1) V_.reset(new Block(c, cap_ + s_ + 1));
     if (!W_ || W_->n() < s_ + 1) W_.reset(new Block(c, s_ + 1));
+    if (prec_ && (!Z_ || Z_->n() < s_ + 1)) Z_.reset(new Block(c, s_ + 1));
     // the pieces of the residual, orthonormalised: rhs = V_1 R_1 (1,..,1)
     int k = Split(rhs);
     for (int i = 0; i < k; i++) {
@@ -888,7 +1037,16 @@ class BlockNewtonKrylov {
     std::vector<double> y;
     for (int j = 0; (j + 1) * bw_ <= cap_; j++) {
       const int nb = (j + 1) * bw_;   // basis vectors so far
-      ApplyJ(x0, *V_, j * bw_, bw_, *W_, 0);
+      if (prec_) {   // right preconditioning: the basis spans J M
+        for (int i = 0; i < bw_; i++) {
+          check(sf_vecs_copy(Z_->v(), i, V_->v(), j * bw_ + i));
+          Z_->p[i] = V_->p[j * bw_ + i];
+        }
+        prec_->Apply(Z_->v(), 0, bw_);
+        ApplyJ(x0, *Z_, 0, bw_, *W_, 0);
+      } else {
+        ApplyJ(x0, *V_, j * bw_, bw_, *W_, 0);
+      }
       used += bw_;
       for (int pass = 0; pass < 2; pass++) {
         std::vector<double> C = block_gram(*V_, 0, nb, *W_, 0, bw_, Ri);
@@ -950,6 +1108,7 @@ class BlockNewtonKrylov {
     for (int i = 0; i < n; i++)
       for (int j = 0; j < n; j++) y[i] += Vv[(size_t)i * n + j] * z[j];
     check(sf_vecs_update(dx.v(), 0, 1, 1.0, V_->v(), 0, n, y.data()));
+    if (prec_) prec_->Apply(dx.v(), 0, 1);
     double p = 0;
     for (int i = 0; i < n; i++) p += y[i] * V_->p[i];
     dx.p = p;
@@ -1116,6 +1275,7 @@ class BlockFixedPoint : public BlockNewtonKrylov {
     EvolveTangentBlock(x0, T_, x0.ctx().p.Ri, k, V, a, k, W, b);
     subtract_identity(V, a, k, W, b);
   }
+  double PreconditionerTime() const override { return T_; }
 
  private:
   double T_;
@@ -1154,6 +1314,7 @@ class BlockPeriodicOrbit : public BlockNewtonKrylov {
     (void)x; (void)F;
     f0_ = std::move(last_f_);
   }
+  double PreconditionerTime() const override { return ref_.p; }
   void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
     Context& c = x0.ctx();
     EvolveTangentBlock(x0, x0.p, c.p.Ri, k, V, a, k, W, b);
@@ -1200,6 +1361,7 @@ class BlockPseudoArclength : public BlockNewtonKrylov {
     phi.p = 0;
     dphi_dri_.reset(new Vec(phi));
   }
+  double PreconditionerTime() const override { return T_; }
   void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
     Context& c = x0.ctx();
     EvolveTangentBlock(x0, T_, x0.p, k, V, a, k, W, b);
