@@ -135,6 +135,11 @@ int sf_step_linear(sf_solver* s, int nsteps);
  * perturbation in run r. nbase must divide nrun; 0 switches it off. */
 int sf_set_tangent(sf_solver* s, int nbase);
 
+/* Launch tuning of the x pass (no counterpart in the reference): the number
+ * of consecutive z-slabs one block walks through (0: chosen from the grid
+ * size). The results do not depend on it. */
+int sf_set_xpass_slabs(sf_solver* s, int slabs);
+
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 

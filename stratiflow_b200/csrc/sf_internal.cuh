@@ -71,6 +71,7 @@ struct StageArgs {
   int tlm;          // tangent-linear batch: runs < tlm are nonlinear bases, run r >= tlm
                     // is linearised about the current state of run (r - tlm) % tlm
   int run_offset;   // first run of this launch (x pass)
+  int xslabs;       // slabs per x-pass block (0: chosen by the launcher)
   float h, hz, hb, cv, cb, pm;
 };
 

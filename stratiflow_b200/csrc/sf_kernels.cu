@@ -13,6 +13,7 @@
 // Every kernel touches only kept (dealiased) modes, which is all the reference's
 // ModalField arithmetic touches (Field.h:1129-1166).
 
+#include <algorithm>
 #include "sf_internal.cuh"
 #include "sf_fft.cuh"
 
@@ -131,9 +132,16 @@ __device__ __forceinline__ int hat_row(int p, int s, int S) {
   return base + s - f;
 }
 
+// products whose first slot repeats the last (Q products) or next-to-last
+// (P4) slot of the slab below; a block that walks up through several slabs
+// keeps those transformed rows instead of forming them again
+__host__ __device__ __forceinline__ bool carried(int p) {
+  return p == P_Q1 || p == P_QB || p == P_Q2 || p == P_P4;
+}
+
 struct XLayout {  // shared-memory carve-up of k_xpass
   int nprod, nrows;
-  size_t hat_off, buf_off, nod_off, base_off, bytes;
+  size_t hat_off, buf_off, nod_off, base_off, carry_off, bytes;
 };
 
 __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int ngroups,
@@ -151,6 +159,7 @@ __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int
   L.buf_off = off;  off += sizeof(float2) * (size_t)ngroups * bufstride;
   L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
+  L.carry_off = off; off += sizeof(float2) * (size_t)4 * K1;   // transformed rows kept for the next slab
   L.bytes = off;
   return L;
 }
@@ -260,11 +269,15 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
 
-// One block per (slab of S output levels, y row, run). Lane groups of G
-// lanes each run one transform at a time; all groups of the block step
-// through their task lists in lockstep so every lane reaches every warp sync.
+// One block per (`iters` consecutive slabs of S output levels, y row, run).
+// Lane groups of G lanes each run one transform at a time; all groups of the
+// block step through their task lists in lockstep so every lane reaches
+// every warp sync. Walking up from one slab to the next, the block keeps the
+// two top nodal levels and the top transformed rows of the carried products
+// (their z stencils reach one level across the slab boundary), so each level
+// is transformed once rather than once per slab that touches it.
 template <int N1, bool LINEAR>
-__global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
+__global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int iters) {
   constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, BUF = fft_buf_stride<N1>();
   const int NGB = blockDim.x / G;   // lane groups per block
   const Geo g = a.g;
@@ -276,7 +289,6 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
   const int K1 = g.K1, N3 = g.N3;
-  const int j0 = blockIdx.x * S;
   const int y = blockIdx.y;
   const int run = blockIdx.z + a.run_offset;
   const int brun = tlm ? (run - tlm) % tlm : run;   // run that holds the base state
@@ -286,13 +298,20 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   const float* zc = a.zc;
   const int NS = S + 2;
   const int nf = tlm ? 8 : 4;   // own u1,u2,u3,b (and the base run's)
+  float2* carry = reinterpret_cast<float2*>(xsm + L.carry_off);   // [4][K1]: Q1, QB, Q2, P4
 
-  // ---- stage the input rows (u1,u2,u3,b at levels j0-1 .. j0+S) ----
-  for (int i = threadIdx.x; i < nf * NS * K1; i += blockDim.x) {
-    const int fb = i / (NS * K1), r = i - fb * NS * K1, s = r / K1, k = r - s * K1;
+  for (int it = 0; it < iters; it++) {
+  const int j0 = (blockIdx.x * iters + it) * S;
+  if (j0 >= N3) break;
+  const int s0 = it == 0 ? 0 : 2;   // nodal slots 0, 1 come from the slab below
+  const int NSn = NS - s0;
+
+  // ---- stage the input rows (u1,u2,u3,b at levels j0-1+s0 .. j0+S) ----
+  for (int i = threadIdx.x; i < nf * NSn * K1; i += blockDim.x) {
+    const int fb = i / (NSn * K1), r = i - fb * NSn * K1, s = s0 + r / K1, k = r - (s - s0) * K1;
     const int f = fb & 3, rr = fb < 4 ? run : brun;
     const int t = j0 - 1 + s;
-    float2* d = stg + i;
+    float2* d = stg + ((size_t)fb * NS + s) * K1 + k;
     if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
       *d = make_float2(0.f, 0.f);
     } else if (g.dim3) {
@@ -318,11 +337,11 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
 
   // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
   // (and of the base run's fields for a tangent-linear batch)
-  const int ntA = NS * (tlm ? 4 : 2);
+  const int ntA = NSn * (tlm ? 4 : 2);
   for (int base = 0; base < ntA; base += NGB) {
     const int task = base + gid;
     const bool valid = task < ntA;
-    const int s = valid ? task % NS : 0, pr4 = valid ? task / NS : 0;
+    const int s = valid ? s0 + task % NSn : 0, pr4 = valid ? task / NSn : 0;
     const int pr = pr4 & 1, ofs = (pr4 >> 1) * 4;   // ofs 4: base rows
     const int fA = pr == 0 ? 0 : 3;       // u1 | b
     const int fB = pr == 0 ? 2 : 1;       // u3 | u2
@@ -362,8 +381,19 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
   }
   __syncthreads();
 
+  // rows carried over from the slab below (the staging area above overlaid them)
+  if (it > 0)
+    for (int i = threadIdx.x; i < 4 * K1; i += blockDim.x) {
+      const int q = i / K1, k = i - q * K1;
+      const int p = q == 0 ? P_Q1 : (q == 1 ? P_QB : (q == 2 ? P_Q2 : P_P4));
+      if (p < L.nprod) hat[(size_t)hat_row(p, p == P_P4 ? 0 : 1, S) * K1 + k] = carry[i];
+    }
+
   // ---- phase B/C: nodal products, forward transforms in pairs (ToModal) ----
-  const int nprod = L.nprod, nrows = L.nrows;
+  const int nprod = L.nprod;
+  int ncar = 0;
+  for (int p = 0; p < nprod; p++) ncar += carried(p) ? 1 : 0;
+  const int nrows = L.nrows - (it > 0 ? ncar : 0);
   const int ntB = (nrows + 1) / 2;
   const float sc = 0.5f * g.inv_n12;
   for (int base = 0; base < ntB; base += NGB) {
@@ -378,9 +408,11 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
       if (task < ntB && r < nrows) {
         for (int p = 0; p < nprod; p++) {
           int f0, c; prod_slots(p, S, f0, c);
-          if (r < c) { pp[h] = p; ss[h] = f0 + r; break; }
-          r -= c;
+          const int skip = (it > 0 && carried(p)) ? 1 : 0;
+          if (r < c - skip) { pp[h] = p; ss[h] = f0 + skip + r; break; }
+          r -= c - skip;
         }
+        if (pp[h] >= 0) row[h] = hat_row(pp[h], ss[h], S);
         const int t = j0 - 1 + ss[h];
         live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
       }
@@ -453,6 +485,24 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S) {
       m[4 * cs] = c3; m[5 * cs] = c3y; m[6 * cs] = cB; m[7 * cs] = cBy;
     }
   }
+
+  // ---- keep what the next slab shares with this one ----
+  if (it + 1 < iters) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * K1; i += blockDim.x) {
+      const int q = i / K1, k = i - q * K1;
+      const int p = q == 0 ? P_Q1 : (q == 1 ? P_QB : (q == 2 ? P_Q2 : P_P4));
+      if (p < nprod) carry[i] = hat[(size_t)hat_row(p, p == P_P4 ? S : S + 1, S) * K1 + k];
+    }
+    for (int i = threadIdx.x; i < nf * 2 * N1; i += blockDim.x) {   // nodal slots S, S+1 -> 0, 1
+      const int fb = i / (2 * N1), r = i - fb * 2 * N1, sl = r / N1, x = r - sl * N1;
+      float* rows = fb < 4 ? nod : bnod;
+      const int f = fb & 3;
+      rows[((size_t)f * NS + sl) * N1 + x] = rows[((size_t)f * NS + S + sl) * N1 + x];
+    }
+    __syncthreads();
+  }
+  }   // slabs
 }
 
 // ============================================================ z pass ====
@@ -1211,8 +1261,17 @@ static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
     if ((long long)((g.N3 + S - 1) / S) * g.N2 * nruns >= 2 * 148) break;
     S = cand[i];
   }
-  dim3 grid(cdiv(g.N3, S), g.N2, nruns);
-  k_xpass<N1, LIN><<<grid, threads(S), bytes(S), st>>>(a, S);
+  // slabs per block: in 3D as many as keep at least two waves of blocks, up
+  // to 6 (measured at 256 x 128 x 384: 6 slabs 2.5% faster per step than 1,
+  // 12 slower); in 2D one (carrying rows saves transforms but not lockstep
+  // rounds there, and the extra barriers cost more)
+  int iters = 1;
+  while (g.dim3 && iters < 6 && S * (iters + 1) <= g.N3 &&
+         (long long)cdiv(g.N3, S * (iters + 1)) * g.N2 * nruns >= 4 * 148)
+    iters++;
+  if (a.xslabs > 0) iters = std::min<int>(a.xslabs, (int)cdiv(g.N3, S));
+  dim3 grid(cdiv(g.N3, S * iters), g.N2, nruns);
+  k_xpass<N1, LIN><<<grid, threads(S), bytes(S), st>>>(a, S, iters);
 }
 
 static void launch_xpass_runs(const StageArgs& a, bool L, int nruns, cudaStream_t st) {

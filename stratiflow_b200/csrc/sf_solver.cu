@@ -50,6 +50,7 @@ struct sf_solver {
   int cur = 0;                   // index of the current state buffer
   bool base_set = false;
   int tlm = 0;                   // tangent-linear batch (sf_set_tangent)
+  int xslabs = 0;                // slabs per x-pass block (sf_set_xpass_slabs)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -171,6 +172,7 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.linear = linear ? 1 : 0;
   a.tlm = linear ? 0 : s->tlm;
   a.run_offset = 0;
+  a.xslabs = s->xslabs;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -616,6 +618,15 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);
+  return SF_OK;
+}
+
+int sf_set_xpass_slabs(sf_solver* s, int slabs) {
+  if (!s || slabs < 0) return fail(SF_EINVAL, "bad argument");
+  if (slabs != s->xslabs) {
+    s->xslabs = slabs;
+    drop_graphs(s);
+  }
   return SF_OK;
 }
 
