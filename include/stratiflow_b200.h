@@ -123,6 +123,9 @@ int sf_step(sf_solver* s, int nsteps);
  * of TimeStepLinear for one run, modal, reference layout */
 int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const float* u3,
                 const float* b);
+/* SetBackground(u1,u2,u3,b) from a state already on the device in the kept
+ * layout [5][N3][plane] (e.g. an sf_vecs vector); synchronises */
+int sf_set_base_device(sf_solver* s, int run, const void* kept_state);
 
 /* nsteps x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41) */
 int sf_step_linear(sf_solver* s, int nsteps);

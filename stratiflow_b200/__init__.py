@@ -36,7 +36,7 @@ EXPORTS = [
     "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
-    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs",
+    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_base_device",
 ]
 
 
@@ -92,7 +92,7 @@ def load_library(path: str | None = None):
         "sf_net_set_params": [vp, fp], "sf_net_forward": [vp, fp, i, fp], "sf_net_set_data": [vp, fp, fp, i],
         "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
         "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
-        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i],
+        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_base_device": [vp, i, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

@@ -1302,23 +1302,26 @@ static int launch_xpass(const StageArgs& a, cudaStream_t st) {
   return 1;
 }
 
+// nz = runs x fields transformed (blockIdx.z = 4 run + field); a single
+// field of a single run (nz = 1) reads and writes that field only
 template <int N2>
-static void ify_launch(const StageArgs& a, int nrun, cudaStream_t st) {
-  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, nrun * 4), kYThreads, 0, st>>>(a);
+static void ify_launch(const StageArgs& a, int nz, cudaStream_t st) {
+  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, nz), kYThreads, 0, st>>>(a);
 }
 template <int N2>
 static void fy_launch(const StageArgs& a, cudaStream_t st) {
   k_fft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, a.g.nrun * 4), kYThreads, 0, st>>>(a);
 }
-static void launch_ifft_y(const StageArgs& a, int nrun, cudaStream_t st) {
+static void launch_ifft_y_z(const StageArgs& a, int nz, cudaStream_t st) {
   switch (a.g.N2) {
-    case 16: ify_launch<16>(a, nrun, st); break;
-    case 32: ify_launch<32>(a, nrun, st); break;
-    case 64: ify_launch<64>(a, nrun, st); break;
-    case 128: ify_launch<128>(a, nrun, st); break;
-    case 256: ify_launch<256>(a, nrun, st); break;
+    case 16: ify_launch<16>(a, nz, st); break;
+    case 32: ify_launch<32>(a, nz, st); break;
+    case 64: ify_launch<64>(a, nz, st); break;
+    case 128: ify_launch<128>(a, nz, st); break;
+    case 256: ify_launch<256>(a, nz, st); break;
   }
 }
+static void launch_ifft_y(const StageArgs& a, int nrun, cudaStream_t st) { launch_ifft_y_z(a, nrun * 4, st); }
 static void launch_fft_y(const StageArgs& a, cudaStream_t st) {
   switch (a.g.N2) {
     case 16: fy_launch<16>(a, st); break;
@@ -1459,7 +1462,7 @@ int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* 
   a.S = kept_modal;   // treated as field 0 of a one-run state
   a.mixin = reinterpret_cast<float2*>(scratch_mixed);
   a.tw = tw;
-  launch_ifft_y(a, 1, st);
+  launch_ifft_y_z(a, 1, st);   // that field only: the input and the scratch hold one field
   k_base_x<<<dim3(g.N3, g.N2), 32, sizeof(float2) * g.N1, st>>>(g, a.mixin, (long long)g.N2 * g.K1, g.K1,
                                                                 base_out, tw);
   return 2;

@@ -539,6 +539,35 @@ int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const f
   return SF_OK;
 }
 
+int sf_set_base_device(sf_solver* s, int run, const void* kept_state) {
+  if (!s || run < 0 || run >= s->g.nrun || !kept_state) return fail(SF_EINVAL, "bad argument");
+  const Geo& g = s->g;
+  if (!s->base) {
+    CK(cudaMalloc(&s->base, sizeof(float) * (size_t)g.nrun * 4 * g.N3 * g.N2 * g.N1));
+    CK(cudaMemset(s->base, 0, sizeof(float) * (size_t)g.nrun * 4 * g.N3 * g.N2 * g.N1));
+    drop_graphs(s);   // graphs captured before hold a null base pointer
+  }
+  float* scratch = nullptr;
+  if (g.dim3) CK(cudaMalloc(&scratch, sizeof(float2) * g.mblk));
+  const float2* src = static_cast<const float2*>(kept_state);
+  for (int f = 0; f < 4; f++) {
+    float* dst = s->base + ((size_t)run * 4 + f) * g.N3 * g.N2 * g.N1;
+    if (f == 1 && !g.dim3) {
+      CK(cudaMemsetAsync(dst, 0, sizeof(float) * (size_t)g.N3 * g.N2 * g.N1, s->st));
+      continue;
+    }
+    // through the same staging buffer as sf_set_base (the 3D transform reads
+    // a whole state's worth of rows from its input)
+    CK(cudaMemcpyAsync(s->qbuf, src + (size_t)f * g.fblk, sizeof(float2) * g.fblk, cudaMemcpyDeviceToDevice, s->st));
+    s->launches += launch_base_nodal(g, s->qbuf, f, dst, s->tw, scratch, s->st);
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s->st));
+  if (scratch) cudaFree(scratch);
+  s->base_set = true;
+  return SF_OK;
+}
+
 int sf_energy(sf_solver* s, int run, double* ke, double* pe) {
   if (!s || run < 0 || run >= s->g.nrun) return fail(SF_EINVAL, "bad argument");
   const Geo& g = s->g;
