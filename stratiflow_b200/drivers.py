@@ -33,6 +33,8 @@ def load_host():
         L.sfh_arclength.argtypes = [dp, i, d, fp, d, fp, d, d, fp, d, dp, fp, dp, dp, i]
         L.sfh_evolve.argtypes = [dp, i, d, d, fp, fp]
         L.sfh_evolve_tangent.argtypes = [dp, i, d, d, fp, fp, fp]
+        L.sfh_arnoldi.argtypes = [dp, fp, d, i, i, d, i, C.c_ulonglong, dp, dp, i, C.POINTER(i), fp, fp, dp]
+        L.sfh_arnoldi.restype = C.c_int
         for f in ("sfh_newton_fixed", "sfh_periodic_orbit", "sfh_arclength", "sfh_evolve", "sfh_evolve_tangent"):
             getattr(L, f).restype = C.c_int
         _host = L
@@ -178,6 +180,28 @@ def evolve_tangent(flow: Flow, x, dx, tau, Ri=None, M=1):
     _call(L.sfh_evolve_tangent(_dp(flow.array()), M, float(tau), float(flow.Ri if Ri is None else Ri), _fp(xs),
                                _fp(ds), _fp(out)))
     return out
+
+
+def arnoldi(flow: Flow, about, T=11.0, block=16, krylov=320, tol=1e-6, nev=6, seed=1, vectors=False):
+    """Eigenvalues (by decreasing modulus) of the linearised evolution over T
+    about the state `about` (BasicArnoldi, Arnoldi.h:15-226; LinearEvolve,
+    StateVector.cpp:107-155), with `block` directions per batched
+    integration. With vectors=True also the real and imaginary parts of the
+    leading eigenvector. Returns (eigenvalues, [vec_re, vec_im,] stats)."""
+    L = load_host()
+    x = np.ascontiguousarray(np.asarray(about, dtype=np.complex64).reshape(flow.state_shape))
+    cap = 4096
+    re, im = np.zeros(cap), np.zeros(cap)
+    n = C.c_int()
+    st = np.zeros(3)
+    vr = np.zeros(flow.state_shape, dtype=np.complex64) if vectors else None
+    vi = np.zeros(flow.state_shape, dtype=np.complex64) if vectors else None
+    _call(L.sfh_arnoldi(_dp(flow.array()), _fp(x), float(T), int(block), int(krylov), float(tol), int(nev), int(seed),
+                        _dp(re), _dp(im), cap, C.byref(n), _fp(vr) if vectors else None,
+                        _fp(vi) if vectors else None, _dp(st)))
+    ev = re[:n.value] + 1j * im[:n.value]
+    stats = {"directions": int(st[0]), "integrations": int(st[1]), "seconds": float(st[2])}
+    return (ev, vr, vi, stats) if vectors else (ev, stats)
 
 
 # ------------------------------------------------------------ continuation

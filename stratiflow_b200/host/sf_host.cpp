@@ -3,6 +3,7 @@
 //   sfh_newton_fixed     BasicNewtonKrylov (BasicNewtonKrylov.h): Phi_T(x) = x
 //   sfh_periodic_orbit   FindPeriodic (FindPeriodic.cpp): Phi_T(x) = x, T unknown
 //   sfh_arclength        one corrector of PseudoArclength (PseudoArclength.cpp:63-68)
+//   sfh_arnoldi          BasicArnoldi (Arnoldi.h:15-226): eigenvalues of the linearised evolution
 // States cross this interface in the kept layout of include/stratiflow_b200.h,
 // M consecutive states (the shooting segments).
 #include <cstring>
@@ -225,6 +226,42 @@ int sfh_evolve_tangent(const double* params, int M, double tau, double Ri, const
     load(d, dx, p);
     EvolveTangent(a, d, tau, Ri, y);
     store(y, out, p);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// Arnoldi (Arnoldi.h, BasicArnoldi) about the state `about` over T: up to
+// nev_cap eigenvalues (by decreasing modulus) into ev_re/ev_im, their number
+// into *nev_out; the leading eigenvector's real and imaginary parts into
+// vec_re/vec_im (kept layout; may be NULL). stats: [0] directions integrated,
+// [1] batched integrations, [2] seconds.
+int sfh_arnoldi(const double* params, const float* about, double T, int block, int krylov, double tol, int nev,
+                unsigned long long seed, double* ev_re, double* ev_im, int nev_cap, int* nev_out, float* vec_re,
+                float* vec_im, double* stats) {
+  try {
+    Params p = params_from(params);
+    Context c(p, 1);
+    Vec x(c), er(c), ei(c);
+    load(x, about, p);
+    x.EnforceBCs();
+    BlockArnoldi ar(block, krylov, tol, nev, seed);
+    ArnoldiResult r = ar.Run(x, T, vec_re ? &er : nullptr, vec_im ? &ei : nullptr);
+    const int n = std::min((int)r.eigenvalues.size(), nev_cap);
+    for (int i = 0; i < n; i++) {
+      ev_re[i] = r.eigenvalues[i].real();
+      ev_im[i] = r.eigenvalues[i].imag();
+    }
+    if (nev_out) *nev_out = n;
+    if (vec_re) store(er, vec_re, p);
+    if (vec_im) store(ei, vec_im, p);
+    if (stats) {
+      stats[0] = r.vectors;
+      stats[1] = (double)r.integrations;
+      stats[2] = r.seconds;
+    }
     return 0;
   } catch (const std::exception& e) {
     g_host_err = e.what();

@@ -16,8 +16,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cmath>
+#include <complex>
 #include <functional>
 #include <memory>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -662,6 +664,47 @@ inline void block_update(Block& B, int b, int nb, double alpha, const Block& A, 
   }
 }
 
+// dst[b..b+k) = src[a..a+k) L^-T with G = L L^T the Gram matrix of the
+// source (FP64); false if it is rank deficient. R = L^T.
+inline bool cholqr(const Block& src, int a, Block& dst, int b, int k, double Ri, std::vector<double>& R) {
+  std::vector<double> G = block_gram(src, a, k, src, a, k, Ri), L;
+  if (!cholesky(G, k, L)) return false;
+  std::vector<double> C((size_t)k * k, 0.0);   // C = L^-T, column by column
+  for (int j = 0; j < k; j++)
+    for (int i = k - 1; i >= 0; i--) {
+      double t = (i == j) ? 1.0 : 0.0;
+      for (int m = i + 1; m < k; m++) t -= L[(size_t)m * k + i] * C[(size_t)m * k + j];
+      C[(size_t)i * k + j] = t / L[(size_t)i * k + i];
+    }
+  check(sf_vecs_scale(dst.v(), b, 0.0, k));
+  for (int i = 0; i < k; i++) dst.p[b + i] = 0.0;
+  block_update(dst, b, k, 1.0, src, a, k, C);
+  R.assign((size_t)k * k, 0.0);
+  for (int i = 0; i < k; i++)
+    for (int j = 0; j < k; j++) R[(size_t)i * k + j] = L[(size_t)j * k + i];
+  return true;
+}
+
+// two passes of Cholesky QR: dst[b..b+k) orthonormal, src = dst R (R = R2 R1);
+// src is overwritten
+inline bool cholqr2(Block& src, int a, Block& dst, int b, int k, double Ri, std::vector<double>& R) {
+  std::vector<double> R1, R2;
+  if (!cholqr(src, a, dst, b, k, Ri, R1)) return false;
+  if (!cholqr(dst, b, src, a, k, Ri, R2)) return false;
+  for (int i = 0; i < k; i++) {
+    check(sf_vecs_copy(dst.v(), b + i, src.v(), a + i));
+    dst.p[b + i] = src.p[a + i];
+  }
+  R.assign((size_t)k * k, 0.0);
+  for (int i = 0; i < k; i++)
+    for (int j = 0; j < k; j++) {
+      double t = 0;
+      for (int m = 0; m < k; m++) t += R2[(size_t)i * k + m] * R1[(size_t)m * k + j];
+      R[(size_t)i * k + j] = t;
+    }
+  return true;
+}
+
 // Evolve's derivative at x0 over tau applied to V[a..a+k) into W[b..b+k):
 // one batched integration of the base and k tangent-linear runs
 // (sf_set_tangent); the scalars of W are zeroed
@@ -955,47 +998,8 @@ class BlockNewtonKrylov {
     return n;
   }
 
-  // dst[b..b+k) = src[a..a+k) L^-T with G = L L^T the Gram matrix of the
-  // source; returns false if it is rank deficient. R = L^T.
-  bool CholQR(const Block& src, int a, Block& dst, int b, int k, double Ri, std::vector<double>& R) {
-    std::vector<double> G = block_gram(src, a, k, src, a, k, Ri), L;
-    if (!cholesky(G, k, L)) return false;
-    // Linv^T: solve L^T X = I column by column -> C[i][j] = (L^-T)[i][j]
-    std::vector<double> C((size_t)k * k, 0.0);
-    for (int j = 0; j < k; j++) {   // column j of L^-T: solve L^T c = e_j
-      for (int i = k - 1; i >= 0; i--) {
-        double t = (i == j) ? 1.0 : 0.0;
-        for (int m = i + 1; m < k; m++) t -= L[(size_t)m * k + i] * C[(size_t)m * k + j];
-        C[(size_t)i * k + j] = t / L[(size_t)i * k + i];
-      }
-    }
-    check(sf_vecs_scale(dst.v(), b, 0.0, k));
-    for (int i = 0; i < k; i++) dst.p[b + i] = 0.0;
-    block_update(dst, b, k, 1.0, src, a, k, C);
-    R.assign((size_t)k * k, 0.0);
-    for (int i = 0; i < k; i++)
-      for (int j = 0; j < k; j++) R[(size_t)i * k + j] = L[(size_t)j * k + i];
-    return true;
-  }
-
-  // two passes of CholQR from W[0..k) into V[at..at+k), R = R2 R1
-  bool CholQR2(int at, int k, double Ri, std::vector<double>& R) {
-    std::vector<double> R1, R2;
-    if (!CholQR(*W_, 0, *V_, at, k, Ri, R1)) return false;
-    if (!CholQR(*V_, at, *W_, 0, k, Ri, R2)) return false;
-    for (int i = 0; i < k; i++) {
-      check(sf_vecs_copy(V_->v(), at + i, W_->v(), i));
-      V_->p[at + i] = W_->p[i];
-    }
-    R.assign((size_t)k * k, 0.0);
-    for (int i = 0; i < k; i++)
-      for (int j = 0; j < k; j++) {
-        double t = 0;
-        for (int m = 0; m < k; m++) t += R2[(size_t)i * k + m] * R1[(size_t)m * k + j];
-        R[(size_t)i * k + j] = t;
-      }
-    return true;
-  }
+  // two passes of Cholesky QR from W[0..k) into V[at..at+k)
+  bool CholQR2(int at, int k, double Ri, std::vector<double>& R) { return cholqr2(*W_, 0, *V_, at, k, Ri, R); }
 
   // least squares min |b0 - H y| over the first n columns
   double Residual(int n, std::vector<double>& y) {
@@ -1376,6 +1380,287 @@ class BlockPseudoArclength : public BlockNewtonKrylov {
   Vec x0c_, v_;
   double ds_, T_;
   std::unique_ptr<Vec> last_phi_, dphi_dri_;
+};
+
+// -------------------------------------------------------------- Arnoldi ----
+// eigenvalues of a real n x n matrix (row-major): Householder reduction to
+// upper Hessenberg form, then the complex QR algorithm with Wilkinson shifts
+// and deflation (Golub & Van Loan, Matrix Computations, 7.4-7.5)
+inline std::vector<std::complex<double>> eigenvalues(std::vector<double> A, int n) {
+  using cd = std::complex<double>;
+  for (int k = 0; k + 2 < n; k++) {   // Hessenberg reduction
+    double nrm = 0;
+    for (int i = k + 1; i < n; i++) nrm += A[(size_t)i * n + k] * A[(size_t)i * n + k];
+    nrm = std::sqrt(nrm);
+    if (nrm == 0) continue;
+    const double a0 = A[(size_t)(k + 1) * n + k];
+    const double alpha = a0 > 0 ? -nrm : nrm;
+    std::vector<double> v(n - k - 1);
+    for (int i = k + 1; i < n; i++) v[i - k - 1] = A[(size_t)i * n + k];
+    v[0] -= alpha;
+    double vn = 0;
+    for (double t : v) vn += t * t;
+    if (vn == 0) continue;
+    for (int j = 0; j < n; j++) {   // A = (I - 2vv'/v'v) A
+      double d = 0;
+      for (int i = k + 1; i < n; i++) d += v[i - k - 1] * A[(size_t)i * n + j];
+      d = 2 * d / vn;
+      for (int i = k + 1; i < n; i++) A[(size_t)i * n + j] -= d * v[i - k - 1];
+    }
+    for (int i = 0; i < n; i++) {   // A = A (I - 2vv'/v'v)
+      double d = 0;
+      for (int j = k + 1; j < n; j++) d += A[(size_t)i * n + j] * v[j - k - 1];
+      d = 2 * d / vn;
+      for (int j = k + 1; j < n; j++) A[(size_t)i * n + j] -= d * v[j - k - 1];
+    }
+  }
+  std::vector<cd> H((size_t)n * n);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) H[(size_t)i * n + j] = (j >= i - 1) ? cd(A[(size_t)i * n + j], 0.0) : cd(0.0);
+  std::vector<cd> ev;
+  int hi = n - 1, iter = 0;
+  while (hi >= 0) {
+    if (hi == 0) {
+      ev.push_back(H[0]);
+      break;
+    }
+    int lo = hi;   // find the active block [lo, hi]
+    while (lo > 0) {
+      const double s = std::abs(H[(size_t)lo * n + lo]) + std::abs(H[(size_t)(lo - 1) * n + lo - 1]);
+      if (std::abs(H[(size_t)lo * n + lo - 1]) <= 1e-15 * (s > 0 ? s : 1.0)) {
+        H[(size_t)lo * n + lo - 1] = 0;
+        break;
+      }
+      lo--;
+    }
+    if (lo == hi) {
+      ev.push_back(H[(size_t)hi * n + hi]);
+      hi--;
+      iter = 0;
+      continue;
+    }
+    // Wilkinson shift: the eigenvalue of the trailing 2 x 2 block closer to H(hi,hi)
+    const cd a = H[(size_t)(hi - 1) * n + hi - 1], b = H[(size_t)(hi - 1) * n + hi];
+    const cd c = H[(size_t)hi * n + hi - 1], d = H[(size_t)hi * n + hi];
+    const cd tr = a + d, det = a * d - b * c;
+    const cd disc = std::sqrt(tr * tr / 4.0 - det);
+    const cd l1 = tr / 2.0 + disc, l2 = tr / 2.0 - disc;
+    cd mu = std::abs(l1 - d) < std::abs(l2 - d) ? l1 : l2;
+    if (++iter % 11 == 0) mu += std::abs(c);   // exceptional shift
+    if (iter > 60 * n) throw std::runtime_error("eigenvalues: QR iteration did not converge");
+    // one shifted QR step on the block by Givens rotations
+    std::vector<cd> cs(hi - lo), sn(hi - lo);
+    for (int k = lo; k <= hi; k++) H[(size_t)k * n + k] -= mu;
+    for (int k = lo; k < hi; k++) {
+      const cd x = H[(size_t)k * n + k], y = H[(size_t)(k + 1) * n + k];
+      const double r = std::sqrt(std::norm(x) + std::norm(y));
+      const cd cc = r > 0 ? x / r : cd(1.0), ss = r > 0 ? y / r : cd(0.0);
+      cs[k - lo] = cc;
+      sn[k - lo] = ss;
+      for (int j = k; j < n; j++) {   // rows k, k+1 <- G^H [rows]
+        const cd t1 = H[(size_t)k * n + j], t2 = H[(size_t)(k + 1) * n + j];
+        H[(size_t)k * n + j] = std::conj(cc) * t1 + std::conj(ss) * t2;
+        H[(size_t)(k + 1) * n + j] = -ss * t1 + cc * t2;
+      }
+    }
+    for (int k = lo; k < hi; k++) {   // columns k, k+1 <- [cols] G
+      const cd cc = cs[k - lo], ss = sn[k - lo];
+      for (int i = 0; i <= std::min(k + 2, hi); i++) {
+        const cd t1 = H[(size_t)i * n + k], t2 = H[(size_t)i * n + k + 1];
+        H[(size_t)i * n + k] = t1 * cc + t2 * ss;
+        H[(size_t)i * n + k + 1] = -t1 * std::conj(ss) + t2 * std::conj(cc);
+      }
+    }
+    for (int k = lo; k <= hi; k++) H[(size_t)k * n + k] += mu;
+  }
+  return ev;
+}
+
+// a null vector of (A - lambda I), A real n x n, by inverse iteration with
+// complex LU (partial pivoting); unit 2-norm
+inline std::vector<std::complex<double>> eigenvector(const std::vector<double>& A, int n, std::complex<double> lambda) {
+  using cd = std::complex<double>;
+  std::vector<cd> M((size_t)n * n);
+  double scale = 0;
+  for (double t : A) scale = std::max(scale, std::fabs(t));
+  const cd shift = lambda + cd(1e-10 * (scale > 0 ? scale : 1.0), 0.0);
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) M[(size_t)i * n + j] = cd(A[(size_t)i * n + j], 0.0) - (i == j ? shift : cd(0.0));
+  std::vector<int> piv(n);
+  for (int k = 0; k < n; k++) {
+    int p = k;
+    for (int i = k + 1; i < n; i++)
+      if (std::abs(M[(size_t)i * n + k]) > std::abs(M[(size_t)p * n + k])) p = i;
+    piv[k] = p;
+    if (p != k)
+      for (int j = 0; j < n; j++) std::swap(M[(size_t)p * n + j], M[(size_t)k * n + j]);
+    if (std::abs(M[(size_t)k * n + k]) == 0.0) M[(size_t)k * n + k] = 1e-300;
+    for (int i = k + 1; i < n; i++) {
+      const cd f = M[(size_t)i * n + k] / M[(size_t)k * n + k];
+      M[(size_t)i * n + k] = f;
+      for (int j = k + 1; j < n; j++) M[(size_t)i * n + j] -= f * M[(size_t)k * n + j];
+    }
+  }
+  std::vector<cd> x(n, cd(1.0));
+  for (int it = 0; it < 3; it++) {
+    for (int k = 0; k < n; k++) std::swap(x[k], x[piv[k]]);
+    for (int i = 0; i < n; i++)
+      for (int j = 0; j < i; j++) x[i] -= M[(size_t)i * n + j] * x[j];
+    for (int i = n - 1; i >= 0; i--) {
+      for (int j = i + 1; j < n; j++) x[i] -= M[(size_t)i * n + j] * x[j];
+      x[i] /= M[(size_t)i * n + i];
+    }
+    double nrm = 0;
+    for (const cd& t : x) nrm += std::norm(t);
+    nrm = std::sqrt(nrm);
+    for (cd& t : x) t /= nrm;
+  }
+  return x;
+}
+
+struct ArnoldiResult {
+  std::vector<std::complex<double>> eigenvalues;   // by decreasing modulus
+  int vectors = 0;                                  // linearised integrations (directions)
+  long long integrations = 0;                       // batched integrations
+  double seconds = 0;
+};
+
+// Arnoldi (Arnoldi.h:15-193, BasicArnoldi): eigenvalues of the linearised
+// evolution over T about a frozen base state (StateVector::LinearEvolve,
+// StateVector.cpp:107-155), with s directions per batched integration
+// (block Arnoldi; s = 1 is the reference's), FP64 block Gram-Schmidt (CGS2)
+// and Cholesky QR, and the eigenvalues of the block Hessenberg matrix in
+// FP64. It stops when the nev largest Ritz values change by less than tol
+// (relative) from one block to the next, or after `krylov` vectors. With
+// eig_re/eig_im it returns the real and imaginary parts of the leading
+// eigenvector (the reference's eigReal / eigImag).
+class BlockArnoldi {
+ public:
+  BlockArnoldi(int s, int krylov, double tol, int nev, unsigned long long seed = 1)
+      : s_(std::max(1, std::min(s, 32))), K_(krylov), tol_(tol), nev_(nev), seed_(seed) {}
+
+  ArnoldiResult Run(const Vec& about, double T, Vec* eig_re = nullptr, Vec* eig_im = nullptr) {
+    Context& c = about.ctx();
+    if (c.M != 1) throw std::runtime_error("Arnoldi needs one segment (M = 1)");
+    auto t0 = std::chrono::steady_clock::now();
+    const double Ri = c.p.Ri;
+    const int cap = std::max(K_ / s_, 2) * s_;
+    Block V(c, cap + s_), W(c, s_);
+    Solver S(c.p, s_);
+    void* base = nullptr;
+    check(sf_vecs_device(about.v(), 0, &base));
+    for (int r = 0; r < s_; r++) check(sf_set_base_device(S.h(), r, base));
+    const int nsteps = std::max(1, (int)std::ceil(T / c.p.dt - 1e-9));
+    S.set_dt(T / nsteps);
+    // starting block: seeded low-wavenumber excitations (ExciteLowWavenumbers, StateVector.cpp:228-236)
+    Seed(c, W);
+    std::vector<double> R;
+    if (!cholqr2(W, 0, V, 0, s_, Ri, R)) throw std::runtime_error("Arnoldi: degenerate starting block");
+    std::vector<double> H((size_t)(cap + s_) * cap, 0.0);
+    ArnoldiResult res;
+    std::vector<std::complex<double>> prev;
+    int n = 0;
+    for (int j = 0; (j + 1) * s_ <= cap; j++) {
+      const int nb = (j + 1) * s_;
+      // W = L V_j: one batched linearised integration of s directions
+      check(sf_vecs_zero_pressure(V.v(), j * s_, s_));
+      check(sf_vecs_to_run(V.v(), j * s_, S.h(), 0, s_));
+      check(sf_prepare(S.h()));
+      check(sf_step_linear(S.h(), nsteps));
+      check(sf_vecs_from_run(W.v(), 0, S.h(), 0, s_));
+      check(sf_vecs_zero_pressure(W.v(), 0, s_));
+      check(sf_vecs_enforce_bcs(W.v(), 0, s_));
+      for (int i = 0; i < s_; i++) W.p[i] = 0;
+      res.vectors += s_;
+      res.integrations += 1;
+      for (int pass = 0; pass < 2; pass++) {
+        std::vector<double> C = block_gram(V, 0, nb, W, 0, s_, Ri);
+        for (int i = 0; i < nb; i++)
+          for (int q = 0; q < s_; q++) H[(size_t)i * cap + j * s_ + q] += C[(size_t)i * s_ + q];
+        block_update(W, 0, s_, -1.0, V, 0, nb, C);
+      }
+      n = nb;
+      std::vector<double> Rn;
+      const bool ok = nb + s_ <= cap + s_ && cholqr2(W, 0, V, nb, s_, Ri, Rn);
+      if (ok)
+        for (int i = 0; i < s_; i++)
+          for (int q = 0; q < s_; q++) H[(size_t)(nb + i) * cap + j * s_ + q] = Rn[(size_t)i * s_ + q];
+      std::vector<double> Hn((size_t)n * n);
+      for (int i = 0; i < n; i++)
+        for (int q = 0; q < n; q++) Hn[(size_t)i * n + q] = H[(size_t)i * cap + q];
+      std::vector<std::complex<double>> ev = eigenvalues(Hn, n);
+      std::sort(ev.begin(), ev.end(), [](auto x, auto y) { return std::abs(x) > std::abs(y); });
+      double change = 1.0;
+      if (!prev.empty()) {
+        change = 0;
+        for (int k = 0; k < std::min<int>(nev_, (int)std::min(ev.size(), prev.size())); k++)
+          change = std::max(change, std::abs(std::abs(ev[k]) - std::abs(prev[k])) / std::max(std::abs(ev[k]), 1e-300));
+      }
+      if (verbose())
+        std::fprintf(stderr, "Arnoldi: %d vectors, largest |eigenvalue| %.8e, change %.2e\n", n, std::abs(ev[0]),
+                     change);
+      prev = ev;
+      res.eigenvalues = ev;
+      if (!ok || change < tol_) break;
+    }
+    if (eig_re || eig_im) {
+      std::vector<double> Hn((size_t)n * n);
+      for (int i = 0; i < n; i++)
+        for (int q = 0; q < n; q++) Hn[(size_t)i * n + q] = H[(size_t)i * cap + q];
+      std::vector<std::complex<double>> y = eigenvector(Hn, n, res.eigenvalues[0]);
+      std::vector<double> yr(n), yi(n);
+      for (int i = 0; i < n; i++) {
+        yr[i] = y[i].real();
+        yi[i] = y[i].imag();
+      }
+      if (eig_re) {
+        eig_re->Zero();
+        check(sf_vecs_update(eig_re->v(), 0, 1, 1.0, V.v(), 0, n, yr.data()));
+      }
+      if (eig_im) {
+        eig_im->Zero();
+        check(sf_vecs_update(eig_im->v(), 0, 1, 1.0, V.v(), 0, n, yi.data()));
+      }
+    }
+    res.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return res;
+  }
+
+ private:
+  int s_, K_;
+  double tol_;
+  int nev_;
+  unsigned long long seed_;
+
+  void Seed(Context& c, Block& W) {
+    const Params& p = c.p;
+    const int K1 = p.N1 / 3, K2 = p.N2 > 1 ? 2 * (p.N2 / 3) - 1 : 1, Ky = p.N2 > 1 ? p.N2 / 3 : 1;
+    const int plane = (K1 * K2 + 15) / 16 * 16;
+    std::vector<float> h((size_t)2 * 5 * p.N3 * plane);
+    std::mt19937_64 rng(seed_);
+    std::normal_distribution<double> nd(0.0, 1.0);
+    auto zf = vertical_points_fractional(p.L3, p.N3);
+    for (int i = 0; i < W.n(); i++) {
+      std::fill(h.begin(), h.end(), 0.f);
+      for (int f = 0; f < 4; f++) {
+        if (f == 1 && p.N2 == 1) continue;
+        for (int j = 1; j < p.N3 - 1; j++)
+          for (int q = 0; q < K2; q++) {
+            const int ky = q < Ky ? q : q - K2;
+            if (std::abs(ky) >= 8) continue;
+            for (int j1 = 0; j1 < std::min(K1, 8); j1++) {
+              const double w = std::exp(-zf[j] * zf[j]);
+              const size_t o = 2 * (((size_t)f * p.N3 + j) * plane + (size_t)q * K1 + j1);
+              h[o] = (float)(w * nd(rng));
+              h[o + 1] = (j1 == 0 && ky == 0) ? 0.f : (float)(w * nd(rng));
+            }
+          }
+      }
+      check(sf_vecs_set_host(W.v(), i, h.data()));
+      W.p[i] = 0;
+    }
+    check(sf_vecs_enforce_bcs(W.v(), 0, W.n()));
+  }
 };
 
 }  // namespace stratiflow

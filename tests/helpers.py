@@ -20,6 +20,9 @@ CONFIGS = {
     # 2D 256 x 1 x 256 of the Newton-Krylov and continuation cases
     "nk2d": dict(N1=256, N2=1, N3=256, L1=L1_DEFAULT, L2=L1_DEFAULT / 2, L3=10.0, Re=1000.0, Ri=0.12,
                  Pr=1.0, dt=0.01, bg="tanh", fields=("u1", "u3")),
+    # small 2D grid for eigenvalue checks against the oracle
+    "lin2d": dict(N1=64, N2=1, N3=64, L1=L1_DEFAULT, L2=L1_DEFAULT / 2, L3=10.0, Re=1000.0, Ri=0.1,
+                  Pr=1.0, dt=0.01, bg="tanh", fields=("u1", "u3")),
     # reduced 3D grid of the same flow, small enough for the oracle in seconds
     "shear3d_small": dict(N1=64, N2=32, N3=64, L1=L1_DEFAULT, L2=L1_DEFAULT / 2, L3=10.0, Re=4000.0,
                           Ri=0.16, Pr=1.0, dt=0.005, bg="holmboe", fields=("u1", "u2", "u3")),
