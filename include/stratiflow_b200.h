@@ -138,6 +138,26 @@ int sf_step_linear(sf_solver* s, int nsteps);
  * perturbation in run r. nbase must divide nrun; 0 switches it off. */
 int sf_set_tangent(sf_solver* s, int nbase);
 
+/* Nodal fields of one run's state in the reference's nodal layout
+ * (N1*n2 + n1)*N3 + n3, float (Field.h:399-410), field SF_U1..SF_B:
+ * sf_get_nodal is PopulateNodalVariables of that field (IMEXRK.h:141-162);
+ * sf_set_nodal is ToModal with its 1/(N1 N2) and Filter (Field.h:734-769)
+ * into the state. Both synchronise. They read and write .fields files
+ * (IMEXRK::SaveFlow / LoadFlow, IMEXRK.h:415-443). */
+int sf_get_nodal(sf_solver* s, int run, int field, float* host);
+int sf_set_nodal(sf_solver* s, int run, int field, const float* host);
+
+/* The maxima over the nodal grid of |U1 + U_|, |U2|, |U3| of one run's state:
+ * the inputs of IMEXRK::CFL (IMEXRK.h:355-373); synchronises */
+int sf_velocity_maxima(sf_solver* s, int run, double* out3);
+
+/* IMEXRK::CFL's number (IMEXRK.h:355-366) for one run at the current dt
+ * (without the reference's update of dt, which FullEvolve does); and the dt */
+int sf_cfl(sf_solver* s, int run, double* cfl);
+int sf_get_dt(sf_solver* s, double* dt);
+/* the number of runs of the solver's batch */
+int sf_get_runs(sf_solver* s, int* nrun);
+
 /* Launch tuning of the x pass (no counterpart in the reference): the number
  * of consecutive z-slabs one block walks through (0: chosen from the grid
  * size). The results do not depend on it. */

@@ -37,6 +37,7 @@ EXPORTS = [
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
     "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_base_device",
+    "sf_get_nodal", "sf_set_nodal", "sf_velocity_maxima", "sf_cfl", "sf_get_dt", "sf_get_runs",
 ]
 
 
@@ -93,6 +94,8 @@ def load_library(path: str | None = None):
         "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
         "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
         "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_base_device": [vp, i, vp],
+        "sf_get_nodal": [vp, i, i, fp], "sf_set_nodal": [vp, i, i, fp], "sf_velocity_maxima": [vp, i, dp],
+        "sf_cfl": [vp, i, dp], "sf_get_dt": [vp, dp], "sf_get_runs": [vp, C.POINTER(i)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -232,6 +235,69 @@ class IMEXRK:
         arrs = [np.ascontiguousarray(np.asarray(x).reshape(self.modal_shape), dtype=np.complex64)
                 for x in (u1, u2, u3, b)]
         _check(load_library().sf_set_base(self._h, int(run), *[_fptr(x) for x in arrs]))
+
+    # ---- nodal fields, .fields files, CFL ----
+    @property
+    def nodal_shape(self):
+        """The reference's nodal layout (N1 n2 + n1) N3 + n3 as [N2][N1][N3]."""
+        return (self.N2, self.N1, self.N3)
+
+    def get_nodal(self, run, name):
+        out = np.zeros(self.nodal_shape, dtype=np.float32)
+        _check(load_library().sf_get_nodal(self._h, int(run), FIELD[name], _fptr(out)))
+        return out
+
+    def set_nodal(self, run, name, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float32).reshape(self.nodal_shape)
+        _check(load_library().sf_set_nodal(self._h, int(run), FIELD[name], _fptr(a)))
+
+    def SaveFlow(self, run, filename):
+        """IMEXRK::SaveFlow (IMEXRK.h:415-423): the nodal U1, U2, U3, B as raw
+        float32 in the reference's layout, one after the other."""
+        with open(filename, "wb") as f:
+            for name in ("u1", "u2", "u3", "b"):
+                f.write(self.get_nodal(run, name).tobytes())
+
+    def LoadFlow(self, run, filename, two_dimensional=False):
+        """IMEXRK::LoadFlow (IMEXRK.h:425-443): reads the four nodal fields and
+        takes them to modal space (ToModal). A two-dimensional file holds one
+        y-plane per field, repeated along y; U2 is then zero."""
+        per = self.N1 * self.N3 if two_dimensional else self.N1 * self.N2 * self.N3
+        raw = np.fromfile(filename, dtype=np.float32)
+        if raw.size != 4 * per:
+            raise SFError(f"{filename}: {raw.size} floats, expected {4 * per}")
+        for i, name in enumerate(("u1", "u2", "u3", "b")):
+            a = raw[i * per:(i + 1) * per]
+            if two_dimensional:
+                a = np.broadcast_to(a.reshape(1, self.N1, self.N3), self.nodal_shape)
+            if two_dimensional and name == "u2":
+                a = np.zeros(self.nodal_shape, dtype=np.float32)
+            self.set_nodal(run, name, a)
+
+    def velocity_maxima(self, run=0):
+        out = (C.c_double * 3)()
+        _check(load_library().sf_velocity_maxima(self._h, int(run), out))
+        return tuple(out)
+
+    def CFL(self, run=0):
+        """IMEXRK::CFL's number at the current dt (IMEXRK.h:355-366)."""
+        c = C.c_double()
+        _check(load_library().sf_cfl(self._h, int(run), C.byref(c)))
+        return c.value
+
+    def FullEvolve(self, T, target_cfl=0.8, interval=100):
+        """StateVector::FullEvolve's loop (StateVector.cpp:3-84) on the device
+        state: RemoveDivergence(0), then steps whose dt is reset every
+        `interval` steps to bring the CFL number (largest over the runs) to
+        `target_cfl`, the last ones shortened to end exactly at T. Returns
+        {"steps", "t", "dt", "cfl_checks", "seconds"}; deltaT holds the last dt."""
+        from .drivers import load_host
+        st = (C.c_double * 5)()
+        rc = load_host().sfh_full_evolve(self._h, float(T), float(target_cfl), int(interval), st)
+        if rc != 0:
+            raise SFError(load_host().sfh_last_error().decode(errors="replace"))
+        self.deltaT = st[2]
+        return {"steps": int(st[0]), "t": st[1], "dt": st[2], "cfl_checks": int(st[3]), "seconds": st[4]}
 
     def set_xpass_slabs(self, slabs):
         """Slabs per x-pass block (0: automatic); a launch setting only."""

@@ -215,6 +215,9 @@ const float* sf_solver_zc(const sf_solver* s) { return s->zc; }
 float2* sf_solver_state(sf_solver* s, int run) { return s->S[s->cur] + (size_t)run * 5 * s->g.fblk; }
 cudaStream_t sf_solver_stream(const sf_solver* s) { return s->st; }
 const std::vector<double>& sf_solver_z(const sf_solver* s, int which) { return which == 0 ? s->zN : s->zfN; }
+const float2* sf_solver_tw(const sf_solver* s) { return s->tw; }
+const float* sf_solver_ubar(const sf_solver* s, int run) { return s->Ubar + (size_t)run * s->g.N3; }
+void sf_solver_count_launches(sf_solver* s, int n) { s->launches += n; }
 
 extern "C" {
 
@@ -647,6 +650,33 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);
+  return SF_OK;
+}
+
+extern "C" int sf_velocity_maxima(sf_solver* s, int run, double* out3);
+
+int sf_get_runs(sf_solver* s, int* nrun) {
+  if (!s || !nrun) return fail(SF_EINVAL, "bad argument");
+  *nrun = s->g.nrun;
+  return SF_OK;
+}
+
+int sf_get_dt(sf_solver* s, double* dt) {
+  if (!s || !dt) return fail(SF_EINVAL, "bad argument");
+  *dt = s->dt;
+  return SF_OK;
+}
+
+// IMEXRK::CFL (IMEXRK.h:355-366): (max|U1 + U_|/d1 + max|U2|/d2 + max|U3|/d3) dt,
+// d1 = L1/N1, d2 = L2/N2, d3 = z(N3/2+1) - z(N3/2), the smallest gap
+int sf_cfl(sf_solver* s, int run, double* cfl) {
+  if (!s || !cfl) return fail(SF_EINVAL, "bad argument");
+  double m[3];
+  int rc = sf_velocity_maxima(s, run, m);
+  if (rc) return rc;
+  const Geo& g = s->g;
+  const double d1 = s->L1 / g.N1, d2 = s->L2 / g.N2, d3 = s->zN[g.N3 / 2 + 1] - s->zN[g.N3 / 2];
+  *cfl = (m[0] / d1 + (g.dim3 ? m[1] / d2 : 0.0) + m[2] / d3) * s->dt;
   return SF_OK;
 }
 

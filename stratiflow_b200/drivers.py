@@ -35,6 +35,8 @@ def load_host():
         L.sfh_evolve_tangent.argtypes = [dp, i, d, d, fp, fp, fp]
         L.sfh_arnoldi.argtypes = [dp, fp, d, i, i, d, i, C.c_ulonglong, dp, dp, i, C.POINTER(i), fp, fp, dp]
         L.sfh_arnoldi.restype = C.c_int
+        L.sfh_full_evolve.argtypes = [C.c_void_p, d, d, i, dp]
+        L.sfh_full_evolve.restype = C.c_int
         for f in ("sfh_newton_fixed", "sfh_periodic_orbit", "sfh_arclength", "sfh_evolve", "sfh_evolve_tangent"):
             getattr(L, f).restype = C.c_int
         _host = L

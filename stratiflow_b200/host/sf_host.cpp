@@ -269,6 +269,19 @@ int sfh_arnoldi(const double* params, const float* about, double T, int block, i
   }
 }
 
+// FullEvolve with the adaptive time step on an existing solver (all its runs)
+int sfh_full_evolve(sf_solver* solver, double T, double target_cfl, int interval, double* stats) {
+  try {
+    int nrun = 0;
+    check(sf_get_runs(solver, &nrun));
+    FullEvolveAdaptive(solver, nrun, T, target_cfl, interval, stats);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
 // Evolve M segments over T/M each (for the callers' own experiments)
 int sfh_evolve(const double* params, int M, double tau, double Ri, const float* in, float* out) {
   try {

@@ -360,6 +360,47 @@ inline bool cholesky(const std::vector<double>& G, int k, std::vector<double>& L
   return true;
 }
 
+// FullEvolve's time loop (StateVector.cpp:3-84) on a solver's device state:
+// RemoveDivergence(0), then every `interval` steps the CFL number (largest
+// over the runs, IMEXRK::CFL, IMEXRK.h:355-373) resets dt to reach
+// target_cfl, and when fewer than `interval` steps remain dt is shortened so
+// that the run ends exactly at T. stats: steps, t, last dt, CFL checks, seconds.
+inline void FullEvolveAdaptive(sf_solver* h, int nrun, double T, double target_cfl, int interval, double* stats) {
+  auto t0 = std::chrono::steady_clock::now();
+  double dt = 0;
+  check(sf_get_dt(h, &dt));
+  check(sf_prepare(h));
+  double t = 0;
+  long long steps = 0;
+  int checks = 0;
+  while (t + 1e-4 < T) {
+    double cfl = 0;
+    for (int r = 0; r < nrun; r++) {
+      double c = 0;
+      check(sf_cfl(h, r, &c));
+      cfl = std::max(cfl, c);
+    }
+    checks++;
+    if (cfl > 0) dt *= target_cfl / cfl;
+    const double remaining = T - t;
+    const int rs = (int)(remaining / dt) + 1;
+    if (rs < interval) dt = remaining / rs;   // finish exactly at T
+    check(sf_set_dt(h, dt));
+    int k = std::min(interval, std::max(1, (int)std::ceil((T - 1e-4 - t) / dt)));
+    check(sf_step(h, k));
+    t += k * dt;
+    steps += k;
+  }
+  check(sf_synchronize(h));
+  if (stats) {
+    stats[0] = (double)steps;
+    stats[1] = t;
+    stats[2] = dt;
+    stats[3] = checks;
+    stats[4] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+}
+
 // ------------------------------------------------------------ FP64 SVD ----
 // one-sided Jacobi SVD of an m x n matrix (m >= n), row-major A:
 // A = U diag(S) V^T, U m x n, V n x n
