@@ -103,3 +103,33 @@ def test_full_evolve_ends_at_T_with_the_target_cfl():
     st3 = s3.FullEvolve(T, target_cfl=0.8, interval=100)
     n = int(T / dt1) + 1
     assert st3["steps"] == n and abs(st3["dt"] - T / n) <= 1e-6 * T / n
+
+
+def test_load_and_interpolate(tmp_path):
+    """StateVector::LoadAndInterpolate (StateVector.h:275-413): onto the same
+    grid it returns the state (coincident points get weight 1); onto a finer
+    grid each kept mode's z column is the linear interpolation (numpy's
+    np.interp, clamped) of the coarse one at interior levels."""
+    from stratiflow_b200.grid import vertical_points, vertical_points_fractional
+    from stratiflow_b200.regrid import load_and_interpolate
+    cfg, ic, s = _state("kh2d")
+    path = os.path.join(tmp_path, "coarse.fields")
+    s.SaveFlow(0, path)
+    same = gpu_solver(cfg)
+    load_and_interpolate(same, 0, path, cfg["N1"], cfg["N3"])
+    for k in ("u1", "u3", "b"):
+        a, b = same.get_field(0, k), s.get_field(0, k)
+        assert rel_l2(a[..., 2:-2], b[..., 2:-2]) < 1e-6, k
+    fine_cfg = dict(CONFIGS["nk2d"])
+    fine = gpu_solver(fine_cfg)
+    load_and_interpolate(fine, 0, path, cfg["N1"], cfg["N3"])
+    zo, zn = vertical_points_fractional(10.0, cfg["N3"]), vertical_points_fractional(10.0, fine_cfg["N3"])
+    src, dst = s.get_field(0, "u1")[0], fine.get_field(0, "u1")[0]
+    K1 = cfg["N1"] // 3
+    for j1 in range(K1):
+        want = np.interp(zn, zo, src[j1].real) + 1j * np.interp(zn, zo, src[j1].imag)
+        got = dst[j1]
+        sl = slice(2, fine_cfg["N3"] - 2)
+        assert np.allclose(got[sl], want[sl], rtol=1e-5, atol=1e-6 * np.abs(src).max()), j1
+    assert not np.any(dst[K1:])   # modes the coarse grid did not keep stay zero
+    del vertical_points
