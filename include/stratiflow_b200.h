@@ -130,6 +130,14 @@ int sf_set_base_device(sf_solver* s, int run, const void* kept_state);
 /* nsteps x IMEXRK::TimeStepLinear (IMEXRK.cpp:26-41) */
 int sf_step_linear(sf_solver* s, int nsteps);
 
+/* IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126, BuildRHSAdjoint IMEXRK.cpp:260-379,
+ * the mixing objective of UpdateAdjointVariables IMEXRK.h:461-500): one step of
+ * every run's adjoint state backwards, given the direct state at the step's
+ * two ends as device arrays of nrun states in the kept layout [5][N3][plane]
+ * (below = the earlier time, above = the later; u1, u2, u3, b are read).
+ * Two-dimensional grids only in this version (SF_EINVAL otherwise). */
+int sf_step_adjoint(sf_solver* s, const void* below, const void* above);
+
 /* Tangent-linear batch (no counterpart in the reference, whose
  * TimeStepLinear keeps its base frozen, IMEXRK.h:334-352): with nbase > 0,
  * sf_step advances runs 0..nbase-1 by TimeStep and every run r >= nbase by

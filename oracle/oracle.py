@@ -56,6 +56,7 @@ def lib():
             ("sfo_set_base", [vp, dp, dp, dp, dp]), ("sfo_energy", [vp, dp, dp]),
             ("sfo_to_nodal", [vp, dp, dp]), ("sfo_to_modal", [vp, dp, dp]),
             ("sfo_make_ic", [vp, C.c_uint64, d, i, i, i]), ("sfo_set_threads", [i]),
+            ("sfo_step_adjoint", [vp, dp, dp]),
         ]:
             fn = getattr(L, name)
             fn.restype = None
@@ -165,6 +166,15 @@ class Oracle:
         arrs = [np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(self.modal_shape))
                 for a in (u1, u2, u3, b)]
         lib().sfo_set_base(self.h, *[_dp(a.view(np.float64)) for a in arrs])
+
+    def step_adjoint(self, below: dict, above: dict):
+        """IMEXRK::TimeStepAdjoint with the direct state below (earlier) and
+        above (later): dicts of modal u1, u2, u3, b."""
+        def pack(st):
+            return np.ascontiguousarray(np.stack([np.asarray(st[k], dtype=np.complex128).reshape(self.modal_shape)
+                                                  for k in ("u1", "u2", "u3", "b")]))
+        bl, ab = pack(below), pack(above)
+        lib().sfo_step_adjoint(self.h, _dp(bl.view(np.float64)), _dp(ab.view(np.float64)))
 
     def energy(self):
         ke, pe = C.c_double(), C.c_double()

@@ -678,6 +678,152 @@ struct Solver {
     to_modal(prod, ntmp); accum(rB, ntmp, IKX, -1);
   }
 
+  // ---- adjoint step (IMEXRK.h:86-126, 461-500; IMEXRK.cpp:260-379) ----
+  // direct total fields of the current RK substep, modal and nodal
+  std::vector<C> u1T, u2T, u3T, bT, mtmp;
+  std::vector<T> U1T, U2T, U3T, BT, U1F, U2F, U3F, BF, nd1, nd2;
+  T adjK = T(2);
+
+  void adjoint_alloc() {
+    if (!u1T.empty()) return;
+    for (auto* f : {&u1T, &u2T, &u3T, &bT, &mtmp}) f->assign(u1.size(), C(0));
+    for (auto* f : {&U1T, &U2T, &U3T, &BT, &U1F, &U2F, &U3F, &BF, &nd1, &nd2}) f->assign(U1.size(), T(0));
+  }
+
+  // IMEXRK::UpdateAdjointVariables (IMEXRK.h:461-500), the mixing objective's
+  // forcing; J itself is not needed by the step
+  void update_adjoint_variables() {
+    to_nodal(u1T, U1T);
+    if (dim3) to_nodal(u2T, U2T); else std::fill(U2T.begin(), U2T.end(), T(0));
+    to_nodal(u3T, U3T);
+    to_nodal(bT, BT);
+    const size_t o00 = midx(0, 0);
+    std::vector<T> bave(N3), wave(N3);   // HorizontalAverage (Integration.h:38-42)
+    for (int j = 0; j < N3; j++) { bave[j] = bT[o00 + j].real(); wave[j] = u3T[o00 + j].real(); }
+    adjK = T(2);
+    nodal_eval(U3F, [&](size_t o, int j) { return (T(1) / adjK) * (BT[o + j] - bave[j]); });
+    nodal_eval(BF, [&](size_t o, int j) { return (T(1) / adjK) * (U3T[o + j] - wave[j]); });
+    std::fill(U1F.begin(), U1F.end(), T(0));
+    std::fill(U2F.begin(), U2F.end(), T(0));
+  }
+
+  // modal derivative of a direct field, to nodal: mul = IKX (ddx) or
+  // DzND / DzDN (ddz), as in `neumannTemp = ddx(u1_tot); ...ToNodal`
+  enum DerivKind { D_X, D_Y, DZ_ND, DZ_DN };
+  void deriv_nodal(const std::vector<C>& f, DerivKind kd, std::vector<T>& out) {
+    per_kept([&](int n1, int n2, int s) {
+      (void)s;
+      size_t o = midx(n1, n2);
+      for (int j = 0; j < N3; j++) {
+        C v;
+        if (kd == D_X) v = C(0, kx[n1]) * f[o + j];
+        else if (kd == D_Y) v = C(0, ky[n2]) * f[o + j];
+        else if (kd == DZ_ND) v = DzND(&f[o], j);
+        else v = DzDN(&f[o], j);
+        mtmp[o + j] = v;
+      }
+    });
+    to_nodal(mtmp, out);
+  }
+
+  // IMEXRK::BuildRHSAdjoint (IMEXRK.cpp:260-379), 2D and 3D
+  void build_rhs_adjoint() {
+    // adjoint buoyancy
+    nodal_eval(prod, [&](size_t o, int j) { return BF[o + j] + Ri * Dir(&U3[o], j); });
+    BF.swap(prod);
+    // advection of adjoint quantities by the direct flow
+    nodal_eval(prod, [&](size_t o, int j) { return U1[o + j] * U1T[o + j]; });
+    to_modal(prod, ntmp); accum(r1, ntmp, IKX, 1);
+    product_bar_dz(U1, U3T); to_modal(prod, ntmp); accum(r1, ntmp, One, 1);
+    nodal_eval(prod, [&](size_t o, int j) { return Tilde(&U1T[o], j) * U3[o + j]; });
+    to_modal(prod, dtmp);
+    nodal_eval(prod, [&](size_t o, int j) { return Dir(&U3[o], j) * Dir(&U3T[o], j); });
+    to_modal(prod, ntmp);
+    accum(r3, dtmp, IKX, 1); accum_dznd(r3, ntmp, 1);
+    if (dim3) {
+      nodal_eval(prod, [&](size_t o, int j) { return U2[o + j] * U2T[o + j]; });
+      to_modal(prod, ntmp); accum(r2, ntmp, IKY, 1);
+      product_bar_dz(U2, U3T); to_modal(prod, ntmp); accum(r2, ntmp, One, 1);
+      nodal_eval(prod, [&](size_t o, int j) { return Tilde(&U2T[o], j) * U3[o + j]; });
+      to_modal(prod, dtmp); accum(r3, dtmp, IKY, 1);
+      nodal_eval(prod, [&](size_t o, int j) { return U1[o + j] * U2T[o + j]; });
+      to_modal(prod, ntmp); accum(r1, ntmp, IKY, 1);
+      nodal_eval(prod, [&](size_t o, int j) { return U2[o + j] * U1T[o + j]; });
+      to_modal(prod, ntmp); accum(r2, ntmp, IKX, 1);
+    }
+    product_bar_dz(B, U3T); to_modal(prod, ntmp); accum(rB, ntmp, One, 1);
+    if (dim3) {
+      nodal_eval(prod, [&](size_t o, int j) { return B[o + j] * U2T[o + j]; });
+      to_modal(prod, ntmp); accum(rB, ntmp, IKY, 1);
+    }
+    nodal_eval(prod, [&](size_t o, int j) { return B[o + j] * U1T[o + j]; });
+    to_modal(prod, ntmp); accum(rB, ntmp, IKX, 1);
+
+    // extra adjoint terms: (grad u_tot)^T u-adjoint and grad b_tot b-adjoint
+    deriv_nodal(u1T, D_X, nd1);                                   // ddx(u1_tot), Neumann
+    nodal_eval(prod2, [&](size_t o, int j) { return nd1[o + j] * U1[o + j]; });
+    if (dim3) {
+      deriv_nodal(u2T, D_X, nd1);
+      nodal_eval(prod2, [&](size_t o, int j) { return prod2[o + j] + nd1[o + j] * U2[o + j]; });
+    }
+    deriv_nodal(u3T, D_X, nd2);                                   // ddx(u3_tot), Dirichlet
+    nodal_eval(prod, [&](size_t o, int j) { return nd2[o + j] * U3[o + j]; });
+    nodal_eval(U1F, [&](size_t o, int j) { return U1F[o + j] - (prod2[o + j] + Dir(&prod[o], j)); });
+    if (dim3) {
+      deriv_nodal(u1T, D_Y, nd1);
+      nodal_eval(prod2, [&](size_t o, int j) { return nd1[o + j] * U1[o + j]; });
+      deriv_nodal(u2T, D_Y, nd1);
+      nodal_eval(prod2, [&](size_t o, int j) { return prod2[o + j] + nd1[o + j] * U2[o + j]; });
+      deriv_nodal(u3T, D_Y, nd2);
+      nodal_eval(prod, [&](size_t o, int j) { return nd2[o + j] * U3[o + j]; });
+      nodal_eval(U2F, [&](size_t o, int j) { return U2F[o + j] - (prod2[o + j] + Dir(&prod[o], j)); });
+    }
+    deriv_nodal(u1T, DZ_ND, nd2);                                // ddz(u1_tot), Dirichlet
+    nodal_eval(prod2, [&](size_t o, int j) { return nd2[o + j] * Full(&U1[o], j); });
+    if (dim3) {
+      deriv_nodal(u2T, DZ_ND, nd2);
+      nodal_eval(prod2, [&](size_t o, int j) { return prod2[o + j] + nd2[o + j] * Full(&U2[o], j); });
+    }
+    deriv_nodal(u3T, DZ_DN, nd1);                                // ddz(u3_tot), Neumann
+    nodal_eval(U3F, [&](size_t o, int j) { return U3F[o + j] - (prod2[o + j] + Full(&nd1[o], j) * U3[o + j]); });
+    deriv_nodal(bT, D_X, nd1);                                    // ddx(b_tot)
+    nodal_eval(U1F, [&](size_t o, int j) { return U1F[o + j] - nd1[o + j] * B[o + j]; });
+    if (dim3) {
+      deriv_nodal(bT, D_Y, nd1);
+      nodal_eval(U2F, [&](size_t o, int j) { return U2F[o + j] - nd1[o + j] * B[o + j]; });
+    }
+    deriv_nodal(bT, DZ_ND, nd2);                                 // ddz(b_tot), Dirichlet
+    nodal_eval(U3F, [&](size_t o, int j) { return U3F[o + j] - nd2[o + j] * Full(&B[o], j); });
+    // the forcing terms
+    to_modal(U1F, ntmp); accum(r1, ntmp, One, 1);
+    if (dim3) { to_modal(U2F, ntmp); accum(r2, ntmp, One, 1); }
+    to_modal(U3F, dtmp); accum(r3, dtmp, One, 1);
+    to_modal(BF, ntmp); accum(rB, ntmp, One, 1);
+  }
+
+  // IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126): the direct state below (the
+  // earlier time) and above (the later one), modal, reference layout
+  void time_step_adjoint(const std::vector<C>* below, const std::vector<C>* above) {
+    adjoint_alloc();
+    T interpFrac = 0;
+    for (int k = 0; k < 3; k++) {
+      cur_k = k;
+      std::vector<C>* tot[4] = {&u1T, &u2T, &u3T, &bT};
+      for (int f = 0; f < 4; f++)
+        for (size_t i = 0; i < u1.size(); i++) (*tot[f])[i] = (T(1) - interpFrac) * above[f][i] + interpFrac * below[f][i];
+      // u1_tot += U_ through nodal space
+      to_nodal(u1T, U1T);
+      for (size_t i = 0; i < U1T.size(); i++) U1T[i] += Ubar[i % N3];
+      to_modal(U1T, u1T);
+      update_adjoint_variables();
+      explicit_rk(k);
+      build_rhs_adjoint();
+      finish_rhs(k);
+      stage_common_tail(k);
+      interpFrac += h[k] / deltaT;
+    }
+  }
+
   void filter_all() {  // IMEXRK.h:128-139 with Field.h:996-1021
     std::vector<char> keep(N2, 0);
     for (int n2 : keptY) keep[n2] = 1;
@@ -947,6 +1093,28 @@ void sfo_populate_nodal(void* hv) {
 void sfo_filter_all(void* hv) {
   auto* h = (Handle*)hv;
   DISPATCH(h, S->filter_all());
+}
+
+// IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126): below and above hold the direct
+// state's u1, u2, u3, b (modal, reference layout, re/im interleaved), one
+// field after the other
+void sfo_step_adjoint(void* hv, const double* below, const double* above) {
+  auto* h = (Handle*)hv;
+  DISPATCH(h, {
+    using Tt = decltype(S->Ri);
+    using Cc = std::complex<Tt>;
+    const size_t n = S->u1.size();
+    std::vector<Cc> bl[4], ab[4];
+    for (int f = 0; f < 4; f++) {
+      bl[f].resize(n);
+      ab[f].resize(n);
+      for (size_t i = 0; i < n; i++) {
+        bl[f][i] = Cc(Tt(below[2 * (f * n + i)]), Tt(below[2 * (f * n + i) + 1]));
+        ab[f][i] = Cc(Tt(above[2 * (f * n + i)]), Tt(above[2 * (f * n + i) + 1]));
+      }
+    }
+    S->time_step_adjoint(bl, ab);
+  });
 }
 
 // IMEXRK::SetBackground(u1,u2,u3,b) (IMEXRK.h:334-352): the frozen base of

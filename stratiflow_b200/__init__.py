@@ -37,7 +37,7 @@ EXPORTS = [
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
     "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_base_device",
-    "sf_get_nodal", "sf_set_nodal", "sf_velocity_maxima", "sf_cfl", "sf_get_dt", "sf_get_runs",
+    "sf_get_nodal", "sf_set_nodal", "sf_velocity_maxima", "sf_cfl", "sf_get_dt", "sf_get_runs", "sf_step_adjoint",
 ]
 
 
@@ -96,6 +96,7 @@ def load_library(path: str | None = None):
         "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_base_device": [vp, i, vp],
         "sf_get_nodal": [vp, i, i, fp], "sf_set_nodal": [vp, i, i, fp], "sf_velocity_maxima": [vp, i, dp],
         "sf_cfl": [vp, i, dp], "sf_get_dt": [vp, dp], "sf_get_runs": [vp, C.POINTER(i)],
+        "sf_step_adjoint": [vp, vp, vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -298,6 +299,29 @@ class IMEXRK:
             raise SFError(load_host().sfh_last_error().decode(errors="replace"))
         self.deltaT = st[2]
         return {"steps": int(st[0]), "t": st[1], "dt": st[2], "cfl_checks": int(st[3]), "seconds": st[4]}
+
+    def TimeStepAdjoint(self, below, above):
+        """IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126): one step of every run's
+        adjoint state, given the direct states at the step's ends (below the
+        earlier, above the later) as Vecs of nrun states or as host arrays in
+        the kept layout [nrun][5][N3][plane]."""
+        L = load_library()
+        keep = []
+
+        def dev(x):
+            if isinstance(x, Vecs):
+                p = C.c_void_p()
+                _check(L.sf_vecs_device(x._h, 0, C.byref(p)))
+                return p
+            v = Vecs(self, self.nrun)
+            a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.kept_shape)
+            for r in range(self.nrun):
+                v.set(r, a[r])
+            keep.append(v)
+            return dev(v)
+        _check(L.sf_step_adjoint(self._h, dev(below), dev(above)))
+        self.synchronize()
+        del keep
 
     def set_xpass_slabs(self, slabs):
         """Slabs per x-pass block (0: automatic); a launch setting only."""

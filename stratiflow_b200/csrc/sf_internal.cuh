@@ -72,6 +72,9 @@ struct StageArgs {
                     // is linearised about the current state of run (r - tlm) % tlm
   int run_offset;   // first run of this launch (x pass)
   int xslabs;       // slabs per x-pass block (0: chosen by the launcher)
+  int adjoint;      // adjoint step: no linear buoyancy terms in the z solve
+  const float2* adir;   // adjoint step: the direct total state of the substep [nrun][4][N3][Pp]
+  float adj_invK;       // adjoint step: 1/K of the mixing objective (IMEXRK.h:487)
   float h, hz, hb, cv, cb, pm;
 };
 
@@ -82,6 +85,13 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev = nullptr)
 int stage_kernel_count(const Geo& g);
 const char* stage_kernel_name(const Geo& g, int i);
 int launch_project(const StageArgs& a, cudaStream_t st);  // RemoveDivergence only
+int launch_z_solves(const StageArgs& a, cudaStream_t st);   // CN solve + RemoveDivergence
+// TimeStepAdjoint's stage (sf_adjoint.cu): the direct state of the substep
+// into a.adir, then the adjoint x pass and the z solves; 2D
+int launch_stage_adjoint(StageArgs a, const float2* below, const float2* above, float frac, float2* adir,
+                         cudaStream_t st);
+size_t adjoint_smem_needed(const Geo& g);
+int prepare_adjoint_kernels();
 int launch_factor(const Geo& g, const double* bands, const double* kx, const double* ky,
                   double h0, double h1, double h2, double Re, double Pr, float* inv_den,
                   cudaStream_t st);

@@ -599,12 +599,12 @@ __global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
       } else if (f == 2) {
         if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
         pm1 = bp[i];
-        if (j >= 1 && !zmode) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
+        if (j >= 1 && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
         bm1 = bx[i];
       } else {
         const float w1 = bx[i];
         const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
-        rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
+        if (!a.adjoint) rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
         w0 = w1;
       }
       float R = u0;
@@ -788,12 +788,12 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
       } else if (f == 2) {
         if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
         pm1 = bp[i];
-        if (j >= 1 && !zmode) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
+        if (j >= 1 && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
         bm1 = bx[i];
       } else {
         const float w1 = bx[i];
         const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
-        rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
+        if (!a.adjoint) rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
         w0 = w1;
       }
       float R = u0;
@@ -1401,6 +1401,18 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
   launch_project(a, st);
   mark();
   return n + extra;
+}
+
+int launch_z_solves(const StageArgs& a, cudaStream_t st) {
+  const Geo& g = a.g;
+  const int nf = g.dim3 ? 4 : 3;
+  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
+  if (z_chunks(g, nf) == 16)
+    k_z_cn_chunked<16><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+  else
+    k_z_cn_chunked<8><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+  launch_project(a, st);
+  return 2;
 }
 
 int launch_factor(const Geo& g, const double* bands, const double* kx, const double* ky, double h0, double h1,

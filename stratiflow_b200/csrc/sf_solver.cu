@@ -45,6 +45,7 @@ struct sf_solver {
   double *bands = nullptr, *kxd = nullptr, *kyd = nullptr, *red = nullptr;
   float2* tw = nullptr;
   float2* stage_ref = nullptr;   // one field in the reference layout
+  float2* adir = nullptr;        // adjoint step: the direct state of the substep
   std::vector<float> hRi;
   std::vector<double> zN, zfN;   // grid (for inspection)
   int cur = 0;                   // index of the current state buffer
@@ -77,7 +78,7 @@ static void free_all(sf_solver* s) {
   for (int l = 0; l < 2; l++)
     for (int p = 0; p < 2; p++)
       if (s->graph[l][p]) cudaGraphExecDestroy(s->graph[l][p]);
-  void* ptrs[] = {s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
+  void* ptrs[] = {s->adir, s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
                   s->fc, s->inv_den, s->kx, s->ky, s->Ri, s->Ubar, s->dBdz, s->bands, s->kxd, s->kyd,
                   s->red, s->tw, s->stage_ref};
   for (void* p : ptrs)
@@ -263,7 +264,8 @@ int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, s
     }                                                                                              \
   } while (0)
 
-  if (prepare_kernels() != 0) return cleanup_fail(fail(SF_ECUDA, "cudaFuncSetAttribute failed"));
+  if (prepare_kernels() != 0 || prepare_adjoint_kernels() != 0)
+    return cleanup_fail(fail(SF_ECUDA, "cudaFuncSetAttribute failed"));
   CKC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
   const size_t cb = sizeof(float2);
   CKC(cudaMalloc(&s->S[0], cb * nrun * 5 * g.fblk));
@@ -654,6 +656,29 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
 }
 
 extern "C" int sf_velocity_maxima(sf_solver* s, int run, double* out3);
+
+// IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126); below/above: nrun device states
+// in the kept layout [nrun][5][N3][plane] (u1, u2, u3, b used)
+int sf_step_adjoint(sf_solver* s, const void* below, const void* above) {
+  if (!s || !below || !above) return fail(SF_EINVAL, "bad argument");
+  const Geo& g = s->g;
+  if (g.dim3) return fail(SF_EINVAL, "the adjoint step is two-dimensional in this version");
+  if (!s->adir) CK(cudaMalloc(&s->adir, sizeof(float2) * (size_t)4 * g.fblk * g.nrun));
+  float frac = 0.f;
+  int cur = s->cur;
+  for (int k = 0; k < 3; k++) {
+    StageArgs a = stage_args(s, k, cur, false);
+    a.tlm = 0;
+    a.adj_invK = 0.5f;   // 1/K, K = 2 (IMEXRK.h:487)
+    s->launches += launch_stage_adjoint(a, static_cast<const float2*>(below), static_cast<const float2*>(above), frac,
+                                        s->adir, s->st);
+    CK(cudaGetLastError());
+    cur = 1 - cur;
+    frac += s->h[k] / (float)s->dt;   // interpFrac += h[k]/deltaT
+  }
+  s->cur = cur;
+  return SF_OK;
+}
 
 int sf_get_runs(sf_solver* s, int* nrun) {
   if (!s || !nrun) return fail(SF_EINVAL, "bad argument");

@@ -72,14 +72,16 @@ class NKOptions:
     runs multiple shooting. krylov: basis vectors before the solve stops.
     precondition: the block solvers' mean-flow preconditioner (the (0,0)
     profiles of u1 and b relax by diffusion alone and are otherwise the
-    slowest directions for GMRES)."""
+    slowest directions for GMRES). relative: newton_fixed's block solver
+    takes the x shift as an unknown with a phase condition (relative
+    equilibria) instead of removing the phase after each update."""
 
     def __init__(self, max_newton=20, krylov=80, target=1e-6, gmres_tol=0.01, Delta=100.0, fd_eps=3e-4,
-                 jacobian="tangent", block=16, precondition=True):
+                 jacobian="tangent", block=16, precondition=True, relative=False):
         assert jacobian in ("tangent", "fd")
         self.v = np.array([max_newton, krylov, target, gmres_tol, Delta, fd_eps,
-                           0.0 if jacobian == "tangent" else 1.0, block, float(bool(precondition))],
-                          dtype=np.float64)
+                           0.0 if jacobian == "tangent" else 1.0, block, float(bool(precondition)),
+                           float(bool(relative))], dtype=np.float64)
 
 
 def _opts(opts, M):

@@ -37,6 +37,7 @@ NKOptions options_from(const double* o) {
   n.fd_eps = o[5];
   n.tangent = o[6] == 0.0;   // 0: tangent-linear Jacobian actions, 1: finite differences
   n.precondition = o[8] != 0.0;
+  n.relative = o[9] != 0.0;
   return n;
 }
 
@@ -123,7 +124,8 @@ const char* sfh_last_error(void) { return g_host_err.c_str(); }
 // target, gmres_tol, Delta, fd_eps, jacobian (0 tangent-linear, 1 finite
 // differences), block (directions per batched Jacobian action; 0: one, which
 // also allows multiple shooting, M > 1; >= 1 needs M = 1), precondition (block
-// solvers: 1 applies the mean-flow preconditioner)
+// solvers: 1 applies the mean-flow preconditioner), relative (block fixed
+// point: 1 makes the x shift an unknown, p the shift)
 int sfh_newton_fixed(const double* params, int M, double T, int constrain, const float* guess, const double* opts,
                      float* out, double* stats, int stats_cap) {
   try {
@@ -136,6 +138,8 @@ int sfh_newton_fixed(const double* params, int M, double T, int constrain, const
     if (block_from(opts) > 0) {
       BlockFixedPoint nk(options_from(opts), block_from(opts), T, constrain != 0);
       if (constrain) nk.EnforceConstraints(x);
+      x.p = 0;
+      nk.SetReference(x);
       s = nk.Run(x);
     } else {
       FixedPoint nk(options_from(opts), T, constrain != 0);

@@ -457,6 +457,7 @@ struct NKOptions {
   bool tangent = true;        // Jacobian actions by the tangent-linear batch, else by
                               // finite differences (NewtonKrylov.h:218-235)
   bool precondition = true;   // block solvers: the mean-flow preconditioner
+  bool relative = false;      // block fixed point: the x shift as an unknown with a phase condition
 };
 
 struct NKStats {
@@ -1299,32 +1300,89 @@ inline void subtract_identity(const Block& V, int a, int k, Block& W, int b) {
 
 // BasicNewtonKrylov (BasicNewtonKrylov.h:5-14) for Phi_T(x) = x, with the
 // phase and average constraints of PseudoArclength.h:15-20
+//
+// With NKOptions::relative the translation in x, which Phi_T commutes with
+// and which makes J singular, becomes an unknown instead of being removed
+// after each update: unknowns (x, p = sigma), F = S_sigma Phi_T(x) - x with
+// S_sigma the phase shift of StateVector::RemovePhaseShift (mode j1 times
+// e^{i j1 sigma}), and the phase condition F_p = t . (x - x_ref), t the
+// direction of a shift of the initial guess x_ref (a relative equilibrium;
+// sigma = 0 for a steady state).
 class BlockFixedPoint : public BlockNewtonKrylov {
  public:
   BlockFixedPoint(const NKOptions& o, int s, double T, bool constrain)
       : BlockNewtonKrylov(o, s), T_(T), constrain_(constrain) {}
+  void SetReference(const Vec& x) {
+    if (!opt.relative) return;
+    ref_.reset(new Vec(x));
+    tref_.reset(new Vec(ShiftDerivative(x)));
+    tref_->p = 0;
+  }
   Vec EvalFunction(const Vec& at) override {
     Vec phi(at);
     Evolve(at, T_, at.ctx().p.Ri, phi);
+    if (opt.relative && ref_) {
+      double sh = at.p;
+      for (int i = 0; i < phi.M(); i++) check(sf_vecs_phase_shift(phi.v(), i, 1, &sh));
+      last_phi_.reset(new Vec(phi));
+      Vec d(at);
+      d.MulAdd(-1.0, *ref_);
+      phi.MulAdd(-1.0, at);
+      phi.p = SegmentDot(*tref_, d, 0);
+      return phi;
+    }
     phi.MulAdd(-1.0, at);
     phi.p = 0;
     return phi;
   }
   void EnforceConstraints(Vec& at) override {
     if (!constrain_) return;
-    at.RemovePhaseShift();
+    if (!opt.relative) at.RemovePhaseShift();   // else the phase condition fixes the phase
     at.RemoveAverage(0);
     at.RemoveAverage(3);
   }
+  void AtIterate(const Vec& x, const Vec& F) override {
+    (void)x; (void)F;
+    if (opt.relative && last_phi_) {
+      dsigma_.reset(new Vec(ShiftDerivative(*last_phi_)));
+      dsigma_->p = 0;
+    }
+  }
   void ApplyJ(const Vec& x0, const Block& V, int a, int k, Block& W, int b) override {
     EvolveTangentBlock(x0, T_, x0.ctx().p.Ri, k, V, a, k, W, b);
+    if (opt.relative && ref_) {
+      double sh = x0.p;
+      for (int i = 0; i < k; i++) check(sf_vecs_phase_shift(W.v(), b + i, 1, &sh));
+    }
     subtract_identity(V, a, k, W, b);
+    if (opt.relative && dsigma_) {
+      check(sf_vecs_update(W.v(), b, k, 1.0, dsigma_->v(), 0, 1, &V.p[a]));
+      std::vector<double> td(k);
+      check(sf_vecs_gram(V.v(), a, k, tref_->v(), 0, 1, x0.ctx().p.Ri, td.data()));
+      for (int i = 0; i < k; i++) W.p[b + i] = td[i];
+    }
   }
   double PreconditionerTime() const override { return T_; }
 
  private:
   double T_;
   bool constrain_;
+  std::unique_ptr<Vec> ref_, tref_, last_phi_, dsigma_;
+
+  // d/dsigma of S_sigma y at sigma = 0 by a central difference of exact phase
+  // shifts (i j1 y up to (j1 e)^2 / 6)
+  static Vec ShiftDerivative(const Vec& y) {
+    const double e = 1e-3;
+    Vec a(y), b(y);
+    double sp = e, sm = -e;
+    for (int i = 0; i < y.M(); i++) {
+      check(sf_vecs_phase_shift(a.v(), i, 1, &sp));
+      check(sf_vecs_phase_shift(b.v(), i, 1, &sm));
+    }
+    check(sf_vecs_lincomb(a.v(), 0, 1.0 / (2 * e), -1.0 / (2 * e), b.v(), 0, y.M()));
+    a.p = 0;
+    return a;
+  }
 };
 
 // FindPeriodic (FindPeriodic.cpp:4-28): unknowns (x, p = T); F = Phi_T(x) - x,
