@@ -467,6 +467,81 @@ class IMEXRK:
         for k in range(3):
             self._stage(k, True)
 
+    # IMEXRK.h:461-500 (the mixing objective's forcing; J itself is not needed)
+    def UpdateAdjointVariables(self, u1t, u2t, u3t, bt):
+        self.U1_tot = self.ToNodal(u1t)
+        self.U2_tot = self.ToNodal(u2t) if self.dim3 else np.zeros_like(self.U1)
+        self.U3_tot = self.ToNodal(u3t)
+        self.B_tot = self.ToNodal(bt)
+        bAve = bt[0, 0].real          # HorizontalAverage (Integration.h:38-42)
+        wAve = u3t[0, 0].real
+        K = 2.0
+        self.u3Forcing = (1 / K) * (self.B_tot - bAve)
+        self.bForcing = (1 / K) * (self.U3_tot - wAve)
+        self.u1Forcing = np.zeros_like(self.U1)
+        self.u2Forcing = np.zeros_like(self.U1)
+
+    # IMEXRK.cpp:260-379
+    def BuildRHSAdjoint(self, u1t, u2t, u3t, bt):
+        Z, TM, TN = self.Z, self.ToModal, self.ToNodal
+        kxm = self.kx[None, :, None]; kym = self.ky[:, None, None]
+        U1, U2, U3, B = self.U1, self.U2, self.U3, self.B
+        U1T, U2T, U3T = self.U1_tot, self.U2_tot, self.U3_tot
+        self.bForcing = self.bForcing + self.Ri * Z(self.Rdir, U3)
+        nt = TM(U1 * U1T); self._acc(self.r1, kxm * nt)
+        nt = TM(Z(self.DzD, Z(self.Rbar, U1) * U3T)); self._acc(self.r1, nt)
+        dt_ = TM(Z(self.Rtilde, U1T) * U3)
+        nt = TM(Z(self.Rdir, U3) * Z(self.Rdir, U3T))
+        self._acc(self.r3, kxm * dt_ + Z(self.DzN, nt))
+        if self.dim3:
+            nt = TM(U2 * U2T); self._acc(self.r2, kym * nt)
+            nt = TM(Z(self.DzD, Z(self.Rbar, U2) * U3T)); self._acc(self.r2, nt)
+            dt_ = TM(Z(self.Rtilde, U2T) * U3); self._acc(self.r3, kym * dt_)
+            nt = TM(U1 * U2T); self._acc(self.r1, kym * nt)
+            nt = TM(U2 * U1T); self._acc(self.r2, kxm * nt)
+        nt = TM(Z(self.DzD, Z(self.Rbar, B) * U3T)); self._acc(self.rB, nt)
+        if self.dim3:
+            nt = TM(B * U2T); self._acc(self.rB, kym * nt)
+        nt = TM(B * U1T); self._acc(self.rB, kxm * nt)
+        # extra adjoint terms
+        nn2 = TN(kxm * u1t) * U1
+        if self.dim3:
+            nn2 = nn2 + TN(kxm * u2t) * U2
+        self.u1Forcing = self.u1Forcing - (nn2 + Z(self.Rdir, TN(kxm * u3t) * U3))
+        if self.dim3:
+            nn2 = TN(kym * u1t) * U1 + TN(kym * u2t) * U2
+            self.u2Forcing = self.u2Forcing - (nn2 + Z(self.Rdir, TN(kym * u3t) * U3))
+        nd2 = TN(Z(self.DzN, u1t)) * Z(self.Rfull, U1)
+        if self.dim3:
+            nd2 = nd2 + TN(Z(self.DzN, u2t)) * Z(self.Rfull, U2)
+        self.u3Forcing = self.u3Forcing - (nd2 + Z(self.Rfull, TN(Z(self.DzD, u3t))) * U3)
+        self.u1Forcing = self.u1Forcing - TN(kxm * bt) * B
+        if self.dim3:
+            self.u2Forcing = self.u2Forcing - TN(kym * bt) * B
+        self.u3Forcing = self.u3Forcing - TN(Z(self.DzN, bt)) * Z(self.Rfull, B)
+        self._acc(self.r1, TM(self.u1Forcing))
+        if self.dim3:
+            self._acc(self.r2, TM(self.u2Forcing))
+        self._acc(self.r3, TM(self.u3Forcing))
+        self._acc(self.rB, TM(self.bForcing))
+
+    # IMEXRK.h:86-126; below / above: dicts of modal u1, u2, u3, b
+    def TimeStepAdjoint(self, below, above):
+        f = 0.0
+        for k in range(3):
+            tot = {n: (1 - f) * above[n] + f * below[n] for n in ("u1", "u2", "u3", "b")}
+            U1T = self.ToNodal(tot["u1"]) + self.U_
+            tot["u1"] = self.ToModal(U1T)
+            self.UpdateAdjointVariables(tot["u1"], tot["u2"], tot["u3"], tot["b"])
+            self.ExplicitRK(k)
+            self.BuildRHSAdjoint(tot["u1"], tot["u2"], tot["u3"], tot["b"])
+            self.FinishRHS(k)
+            self.CrankNicolson(k)
+            self.RemoveDivergence(1 / self.h[k])
+            self.FilterAll()
+            self.PopulateNodalVariables()
+            f += self.h[k] / self.deltaT
+
     def SetBase(self, u1, u2, u3, b):  # IMEXRK.h:334-352
         self.U1b = self.ToNodal(u1)
         if self.dim3:

@@ -90,6 +90,18 @@ def main():
             imex.TimeStepLinear()
         for k in ("u1", "u2", "u3", "b", "p"):
             out["lin2_" + k] = getattr(imex, k).copy()
+        # two adjoint steps between the prepared input (below) and the
+        # 3-step state (above), from the linear result as the adjoint state
+        below = {k: out["prep_" + k] for k in ("u1", "u2", "u3", "b")}
+        above = {k: out["step3_" + k] for k in ("u1", "u2", "u3", "b")}
+        imex.p[:] = 0
+        imex.Prepare()
+        for k in ("u1", "u2", "u3", "b", "p"):
+            out["adjin_" + k] = getattr(imex, k).copy()
+        for _ in range(2):
+            imex.TimeStepAdjoint(below, above)
+        for k in ("u1", "u2", "u3", "b", "p"):
+            out["adj2_" + k] = getattr(imex, k).copy()
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(name, "written")
 
