@@ -304,15 +304,18 @@ class IMEXRK:
         """IMEXRK::TimeStepAdjoint (IMEXRK.h:86-126): one step of every run's
         adjoint state, given the direct states at the step's ends (below the
         earlier, above the later) as Vecs of nrun states or as host arrays in
-        the kept layout [nrun][5][N3][plane]."""
+        the kept layout [nrun][5][N3][plane]; a (Vecs, i) pair names the nrun
+        states from vector i on."""
         L = load_library()
         keep = []
 
         def dev(x):
-            if isinstance(x, Vecs):
+            if isinstance(x, tuple) and isinstance(x[0], Vecs):
                 p = C.c_void_p()
-                _check(L.sf_vecs_device(x._h, 0, C.byref(p)))
+                _check(L.sf_vecs_device(x[0]._h, int(x[1]), C.byref(p)))
                 return p
+            if isinstance(x, Vecs):
+                return dev((x, 0))
             v = Vecs(self, self.nrun)
             a = np.ascontiguousarray(x, dtype=np.complex64).reshape(self.kept_shape)
             for r in range(self.nrun):
@@ -322,6 +325,27 @@ class IMEXRK:
         _check(L.sf_step_adjoint(self._h, dev(below), dev(above)))
         self.synchronize()
         del keep
+
+    def AdjointEvolve(self, direct0, adjoint_T, steps):
+        """StateVector::AdjointEvolve (StateVector.cpp:158-187) with its direct
+        snapshots: the direct state direct0 (kept layout, all runs) is evolved
+        `steps` fixed steps with every state kept on the device, then the
+        adjoint state adjoint_T is projected and taken back through the steps,
+        each between the stored states at its two ends. The solver holds the
+        adjoint state at the start time afterwards; returns it (kept layout)."""
+        n = self.nrun
+        snaps = Vecs(self, (steps + 1) * n)
+        self.set_state_kept(direct0)
+        self.Prepare()
+        snaps.from_run(0, 0, n)
+        for k in range(steps):
+            self.TimeStep(1)
+            snaps.from_run((k + 1) * n, 0, n)
+        self.set_state_kept(adjoint_T)
+        self.Prepare()
+        for step in range(steps):
+            self.TimeStepAdjoint((snaps, (steps - 1 - step) * n), (snaps, (steps - step) * n))
+        return self.get_state_kept()
 
     def set_xpass_slabs(self, slabs):
         """Slabs per x-pass block (0: automatic); a launch setting only."""
