@@ -32,7 +32,7 @@ __host__ __device__ constexpr int ycols() { return (kYThreads / 32) * (32 / FFTS
 // One lane group per kx column; consecutive columns in consecutive groups so
 // that a warp's loads of one y row cover whole 32-byte sectors.
 template <int N2>
-__global__ void __launch_bounds__(kYThreads) k_ifft_y(StageArgs a) {
+__global__ void __launch_bounds__(kYThreads, 8) k_ifft_y(StageArgs a) {
   constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E, BUF = fft_buf_stride<N2>();
   const Geo g = a.g;
   __shared__ float2 fbuf[(kYThreads / G) * BUF];
@@ -816,8 +816,11 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
     }
   }
   zscan_up<ZW>(sA, sB, sIn, w, lane, A, B);
-  // ---- forward, pass 2: D_j ----
+  // ---- forward, pass 2: D_j, and with it the chunk map of the backward
+  // sweep x_j = D_j - C_j x_{j+1}, composed upwards: x_js = B + A x_je ----
   float D = sIn[w * 32 + lane];
+  A = 1.f;
+  B = 0.f;
   for (int j0 = js; j0 < je; j0 += kZU2) {
     float bi[kZU2];
     load_iden(bi, iden, Pp, j0, 1, js, je);
@@ -828,21 +831,8 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
       const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
       D = al * D + sD[j * 32 + lane];
       sD[j * 32 + lane] = D;
-    }
-  }
-  // ---- backward, pass 1: chunk map of x_j = D_j - C_j x_{j+1} ----
-  A = 1.f;
-  B = 0.f;
-  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
-    float bi[kZU2];
-    load_iden(bi, iden, Pp, j0, -1, js, je);
-#pragma unroll
-    for (int i = 0; i < kZU2; i++) {
-      const int j = j0 - i;
-      if (j < js) break;
-      const float Cj = fc[j] * bi[i];
-      A = -Cj * A;
-      B = -Cj * B + sD[j * 32 + lane];
+      B = B + A * D;
+      A = -A * (fc[j] * bi[i]);
     }
   }
   __syncthreads();
@@ -936,7 +926,15 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
     }
   }
   zscan_up<ZW>(sA, sB, sIn, w, lane, A, B);
+  // D_j, and with it the chunk map of the backward sweep, composed upwards
+  auto Cof = [&](int j, float bij) {
+    float Cj = c_[j] * bij;
+    if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
+    return Cj;
+  };
   float D = sIn[w * 32 + lane];
+  A = 1.f;
+  B = 0.f;
   for (int j0 = js; j0 < je; j0 += kZU2) {
     float bi[kZU2];
     load_iden(bi, iden, Pp, j0, 1, js, je);
@@ -947,26 +945,8 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
       const float al = (j == 0) ? 0.f : -a_[j] * bi[i];
       D = al * D + sD[j * 32 + lane];
       sD[j * 32 + lane] = D;
-    }
-  }
-  // ---- backward: q ----
-  auto Cof = [&](int j, float bij) {
-    float Cj = c_[j] * bij;
-    if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
-    return Cj;
-  };
-  A = 1.f;
-  B = 0.f;
-  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
-    float bi[kZU2];
-    load_iden(bi, iden, Pp, j0, -1, js, je);
-#pragma unroll
-    for (int i = 0; i < kZU2; i++) {
-      const int j = j0 - i;
-      if (j < js) break;
-      const float Cj = Cof(j, bi[i]);
-      A = -Cj * A;
-      B = -Cj * B + sD[j * 32 + lane];
+      B = B + A * D;
+      A = -A * Cof(j, bi[i]);
     }
   }
   __syncthreads();
