@@ -7,9 +7,9 @@
 //                   1/(N1 N2), 2/3 truncation and the z stencils and
 //                   x-derivatives that follow each product
 //   [3D] k_fft_y    (kx, y) -> (kx, ky), y-derivatives, sum into r
-//        k_z_cn     per (mode, field): ExplicitRK + linear buoyancy terms +
-//                   FinishRHS + CrankNicolson right-hand side + Thomas solve
-//        k_z_proj   per mode: divergence, Laplacian solve, projection, p update
+//        k_z_cn_chunked    per (mode, field): ExplicitRK + linear buoyancy terms +
+//                          FinishRHS + CrankNicolson right-hand side + Thomas solve
+//        k_z_proj_chunked  per mode: divergence, Laplacian solve, projection, p update
 // Every kernel touches only kept (dealiased) modes, which is all the reference's
 // ModalField arithmetic touches (Field.h:1129-1166).
 
@@ -506,142 +506,9 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
 }
 
 // ============================================================ z pass ====
-constexpr int kZThreads = 128;
 constexpr int kZU = 8;   // levels of every input loaded ahead per thread
 
 
-// ExplicitRK (IMEXRK.cpp:119-134), the linear terms of BuildRHS (:140-147),
-// FinishRHS (:107-117), CrankNicolson (:75-98) and the Thomas solve
-// (Tridiagonal.h:29-53) for one (run, mode, field, real|imag component):
-// the factors are real, so the real and imaginary parts are independent
-// solves (Field.h:519-531). The forward sweep loads kZU levels of every input
-// into registers before using them, stores D_j in the next state, and the
-// backward sweep overwrites D_j with the solution.
-__global__ void __launch_bounds__(kZThreads) k_z_cn(StageArgs a) {
-  const Geo g = a.g;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int m = t >> 1, c = t & 1;
-  const int run = blockIdx.z;
-  if (m >= g.P) return;
-  const int fi = blockIdx.y;
-  const int f = g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
-  const int N3 = g.N3, Pp = g.Pp;
-  const int q = m / g.K1, j1 = m - q * g.K1;
-  const float kxv = a.kx[j1], kyv = a.ky[q];
-  const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
-  const float sc = c == 0 ? -1.f : 1.f;   // (i k z)_c = sc * k * z_{1-c}
-  const bool dir = (f == 2);
-  const int fam = (f == 3) ? 1 : (dir ? 2 : 0);
-  const int fs = fam * 3 + a.stage;
-  const float* __restrict__ fa = a.fa + (size_t)fs * N3;
-  const float* __restrict__ fc = a.fc + (size_t)fs * N3;
-  const float* __restrict__ iden = a.inv_den + (size_t)fs * N3 * Pp + m;
-  const float* __restrict__ zc = a.zc;
-  const float* __restrict__ lo2 = zc + (dir ? ZC_D2D_LO : ZC_D2N_LO) * N3;
-  const float* __restrict__ di2 = zc + (dir ? ZC_D2D_DI : ZC_D2N_DI) * N3;
-  const float* __restrict__ up2 = zc + (dir ? ZC_D2D_UP : ZC_D2N_UP) * N3;
-  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
-  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
-  const float* __restrict__ full_lo = zc + ZC_FULL_LO * N3;
-  const float* __restrict__ full_di = zc + ZC_FULL_DI * N3;
-  const float cco = (f == 3) ? a.cb : a.cv;
-  const float Ri = a.Ri[run];
-  const float* __restrict__ dB = a.dBdz + (size_t)run * N3;
-  const bool zmode = (m == 0);   // the (0,0) mode: no buoyancy force (IMEXRK.cpp:141-143)
-
-  const float2* __restrict__ u = a.S + ((size_t)(run * 5 + f) * N3) * Pp + m;
-  const float2* __restrict__ pp = a.S + ((size_t)(run * 5 + 4) * N3) * Pp + m;
-  const float2* __restrict__ bsrc = a.S + ((size_t)(run * 5 + 3) * N3) * Pp + m;
-  const float2* __restrict__ u3s = a.S + ((size_t)(run * 5 + 2) * N3) * Pp + m;
-  const float2* __restrict__ rnl = a.rnl + ((size_t)(run * 4 + f) * N3) * Pp + m;
-  float* __restrict__ rold = reinterpret_cast<float*>(a.rold + ((size_t)(run * 4 + f) * N3) * Pp + m) + c;
-  float* __restrict__ out = reinterpret_cast<float*>(a.Sn + ((size_t)(run * 5 + f) * N3) * Pp + m) + c;
-  const float* uc = reinterpret_cast<const float*>(u) + c;
-  const float* pc = reinterpret_cast<const float*>(pp) + c;           // p_c
-  const float* po = reinterpret_cast<const float*>(pp) + (1 - c);     // p_{1-c}
-  const float* bc = reinterpret_cast<const float*>(bsrc) + c;
-  const float* wc = reinterpret_cast<const float*>(u3s) + c;
-  const float* rc = reinterpret_cast<const float*>(rnl) + c;
-  const bool use_rold = (a.hz != 0.f);
-  const float kgrad = (f == 0) ? kxv : kyv;
-
-  float um = 0.f, u0 = uc[0];
-  float pm1 = 0.f, bm1 = 0.f, w0 = wc[0];
-  float Dprev = 0.f;
-  for (int j0 = 0; j0 < N3; j0 += kZU) {
-    float bu[kZU], br[kZU], bo[kZU], bp[kZU], bx[kZU], bi[kZU];
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = j0 + i;
-      const bool in = j < N3, nx = j + 1 < N3;
-      bu[i] = nx ? uc[2 * (size_t)(j + 1) * Pp] : 0.f;
-      br[i] = in ? rc[2 * (size_t)j * Pp] : 0.f;
-      bo[i] = (in && use_rold) ? rold[2 * (size_t)j * Pp] : 0.f;
-      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
-      bp[i] = 0.f;
-      bx[i] = 0.f;
-      if (f <= 1) bp[i] = in ? po[2 * (size_t)j * Pp] : 0.f;
-      if (f == 2) {
-        bp[i] = in ? pc[2 * (size_t)j * Pp] : 0.f;
-        bx[i] = in ? bc[2 * (size_t)j * Pp] : 0.f;
-      }
-      if (f == 3) bx[i] = nx ? wc[2 * (size_t)(j + 1) * Pp] : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = j0 + i;
-      if (j >= N3) break;
-      const float up = bu[i];
-      float rt = br[i];
-      float gp = 0.f;
-      if (f <= 1) {
-        gp = sc * kgrad * bp[i];   // (i k p)_c
-      } else if (f == 2) {
-        if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
-        pm1 = bp[i];
-        if (j >= 1 && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
-        bm1 = bx[i];
-      } else {
-        const float w1 = bx[i];
-        const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
-        if (!a.adjoint) rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
-        w0 = w1;
-      }
-      float R = u0;
-      if (use_rold) R += a.hz * bo[i];
-      R += -a.h * gp;
-      R += a.hb * rt;
-      const bool band = dir ? (j >= 2 && j <= N3 - 2) : (j >= 1 && j <= N3 - 2);
-      const float d2u = band ? lo2[j] * um + di2[j] * u0 + up2[j] * up : 0.f;
-      R += cco * ((d1 * u0 + d2 * u0) + d2u);
-      const bool zend = (j <= 1) || (j >= N3 - 2) || (dir && j == 2);   // ZeroEnds (Field.h:475-486)
-      if (zend) R = 0.f;
-      const float D = (j == 0) ? R * bi[i] : (R - fa[j] * Dprev) * bi[i];
-      out[2 * (size_t)j * Pp] = D;
-      rold[2 * (size_t)j * Pp] = rt;
-      Dprev = D;
-      um = u0;
-      u0 = up;
-    }
-  }
-  float x = Dprev;
-  for (int jt = N3 - 2; jt >= 0; jt -= kZU) {
-    float bd[kZU], bi[kZU];
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = jt - i;
-      bd[i] = j >= 0 ? out[2 * (size_t)j * Pp] : 0.f;
-      bi[i] = j >= 0 ? iden[(size_t)j * Pp] : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = jt - i;
-      if (j < 0) break;
-      x = bd[i] - (fc[j] * bi[i]) * x;
-      out[2 * (size_t)j * Pp] = x;
-    }
-  }
-}
 
 // ------------------------------------------------ chunked z solves ----
 // The Thomas sweeps are first-order affine recurrences: D_j = al_j D_{j-1} +
@@ -979,112 +846,6 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
   }
 }
 
-// RemoveDivergence (IMEXRK.cpp:43-73) for one (run, mode, component):
-// div = ddx u1 + ddy u2 + ddz u3, ZeroEnds, Laplacian Thomas solve,
-// u -= grad q, p += pm q. The two components of a mode sit in adjacent lanes,
-// which exchange q for the x/y gradients. u1,u2,u3 are updated in place in
-// `U`; p is read from `Psrc` and written to `Pdst`. No thread exits before
-// the shuffles: lanes past the last mode work on a clamped copy and store
-// nothing.
-__global__ void __launch_bounds__(kZThreads) k_z_proj(Geo g, float2* U, const float2* Psrc, float2* Pdst,
-                                                   float2* qbuf, const float* zc, const float* fa,
-                                                   const float* fc, const float* inv_den,
-                                                   const float* kx, const float* ky, float pm) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  const int run = blockIdx.z;
-  const bool act = (t >> 1) < g.P;
-  const int m = act ? (t >> 1) : 0, c = t & 1;
-  const int N3 = g.N3, Pp = g.Pp;
-  const int q = m / g.K1, j1 = m - q * g.K1;
-  const float kxv = kx[j1], kyv = g.dim3 ? ky[q] : 0.f;
-  const float sc = c == 0 ? -1.f : 1.f;
-  float* u1 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 0) * N3) * Pp + m);
-  float* u2 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 1) * N3) * Pp + m);
-  float* u3 = reinterpret_cast<float*>(U + ((size_t)(run * 5 + 2) * N3) * Pp + m) + c;
-  const float* ps = reinterpret_cast<const float*>(Psrc + ((size_t)(run * 5 + 4) * N3) * Pp + m) + c;
-  float* pd = reinterpret_cast<float*>(Pdst + ((size_t)(run * 5 + 4) * N3) * Pp + m) + c;
-  float* qb = reinterpret_cast<float*>(qbuf + (size_t)run * N3 * Pp + m) + c;
-  const float* __restrict__ a_ = fa + (size_t)kFS_Lap * N3;
-  const float* __restrict__ c_ = fc + (size_t)kFS_Lap * N3;
-  const float* __restrict__ iden = inv_den + (size_t)kFS_Lap * N3 * Pp + m;
-  const float* __restrict__ ddn_di = zc + ZC_DDN_DI * N3;
-  const float* __restrict__ ddn_up = zc + ZC_DDN_UP * N3;
-  const float* __restrict__ dnd_lo = zc + ZC_DND_LO * N3;
-  const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
-  const float* u1o = u1 + (1 - c);   // u1_{1-c}
-  const float* u2o = u2 + (1 - c);
-  float* u1c = u1 + c;
-  float* u2c = u2 + c;
-
-  float w0 = u3[0];
-  float Dprev = 0.f;
-  for (int j0 = 0; j0 < N3; j0 += kZU) {
-    float b1[kZU], b2[kZU], b3[kZU], bi[kZU];
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = j0 + i;
-      const bool in = j < N3;
-      b1[i] = in ? u1o[2 * (size_t)j * Pp] : 0.f;
-      b2[i] = (in && g.dim3) ? u2o[2 * (size_t)j * Pp] : 0.f;
-      b3[i] = (j + 1 < N3) ? u3[2 * (size_t)(j + 1) * Pp] : 0.f;
-      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = j0 + i;
-      if (j >= N3) break;
-      const float w1 = b3[i];
-      float dv = 0.f;
-      if (j >= 2 && j <= N3 - 3) dv = sc * (kxv * b1[i] + kyv * b2[i]) + (ddn_di[j] * w0 + ddn_up[j] * w1);
-      const float D = (j == 0) ? dv * bi[i] : (dv - a_[j] * Dprev) * bi[i];
-      if (act) qb[2 * (size_t)j * Pp] = D;
-      Dprev = D;
-      w0 = w1;
-    }
-  }
-  // backward sweep: q_j, then u1_j, u2_j, p_j and u3_{j+1}
-  float qn = Dprev;   // q_{N-1}
-  {
-    const int j = N3 - 1;
-    const float qo = __shfl_xor_sync(0xffffffffu, qn, 1);
-    if (act) {
-      u1c[2 * (size_t)j * Pp] -= sc * kxv * qo;
-      if (g.dim3) u2c[2 * (size_t)j * Pp] -= sc * kyv * qo;
-      pd[2 * (size_t)j * Pp] = ps[2 * (size_t)j * Pp] + pm * qn;
-    }
-  }
-  for (int jt = N3 - 2; jt >= 0; jt -= kZU) {
-    float bq[kZU], bi[kZU], b1[kZU], b2[kZU], b3[kZU], bp[kZU];
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = jt - i;
-      const bool in = j >= 0;
-      bq[i] = in ? qb[2 * (size_t)j * Pp] : 0.f;
-      bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
-      b1[i] = in ? u1c[2 * (size_t)j * Pp] : 0.f;
-      b2[i] = (in && g.dim3) ? u2c[2 * (size_t)j * Pp] : 0.f;
-      b3[i] = in ? u3[2 * (size_t)(j + 1) * Pp] : 0.f;
-      bp[i] = in ? ps[2 * (size_t)j * Pp] : 0.f;
-    }
-#pragma unroll
-    for (int i = 0; i < kZU; i++) {
-      const int j = jt - i;
-      if (j < 0) break;
-      float Cj = c_[j] * bi[i];
-      if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
-      const float qj = bq[i] - Cj * qn;
-      const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
-      if (act) {
-        u1c[2 * (size_t)j * Pp] = b1[i] - sc * kxv * qo;
-        if (g.dim3) u2c[2 * (size_t)j * Pp] = b2[i] - sc * kyv * qo;
-        pd[2 * (size_t)j * Pp] = bp[i] + pm * qj;
-        const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
-        if (jj >= 2) u3[2 * (size_t)jj * Pp] = b3[i] - (dnd_lo[jj] * qj + dnd_di[jj] * qn);
-      }
-      qn = qj;
-    }
-  }
-}
 
 // ====================================================== factorisation ====
 // Thomas factors of every (factor set, mode) in FP64 (Tridiagonal.h:14-27):

@@ -103,7 +103,7 @@ __global__ void k_na_grid(int N, double L, double* __restrict__ coef) {
   coef[NA_DND_DI * kNaMaxN3 + j] = ndi;
 }
 
-// The projection of k_z_proj on caller-owned fields [N3][plane] with the
+// The projection of k_z_proj_chunked on caller-owned fields [N3][plane] with the
 // solve's scratch in the fixed array: the Laplacian rows (IMEXRK.h:55-78 with
 // Neumannify) are factorised in FP64 during the forward sweep; D_j and C_j
 // go to the scratch for the backward sweep. Thread per (mode, component);
