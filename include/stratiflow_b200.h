@@ -134,8 +134,7 @@ int sf_step_linear(sf_solver* s, int nsteps);
  * the mixing objective of UpdateAdjointVariables IMEXRK.h:461-500): one step of
  * every run's adjoint state backwards, given the direct state at the step's
  * two ends as device arrays of nrun states in the kept layout [5][N3][plane]
- * (below = the earlier time, above = the later; u1, u2, u3, b are read).
- * Two-dimensional grids only in this version (SF_EINVAL otherwise). */
+ * (below = the earlier time, above = the later; u1, u2, u3, b are read). */
 int sf_step_adjoint(sf_solver* s, const void* below, const void* above);
 
 /* Tangent-linear batch (no counterpart in the reference, whose

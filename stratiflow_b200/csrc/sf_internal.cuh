@@ -74,6 +74,7 @@ struct StageArgs {
   int xslabs;       // slabs per x-pass block (0: chosen by the launcher)
   int adjoint;      // adjoint step: no linear buoyancy terms in the z solve
   const float2* adir;   // adjoint step: the direct total state of the substep [nrun][4][N3][Pp]
+  float2* amix;         // 3D adjoint step: 12 y-transformed fields [nrun][12][N3][N2][K1]
   float adj_invK;       // adjoint step: 1/K of the mixing objective (IMEXRK.h:487)
   float h, hz, hb, cv, cb, pm;
 };
@@ -86,6 +87,7 @@ int stage_kernel_count(const Geo& g);
 const char* stage_kernel_name(const Geo& g, int i);
 int launch_project(const StageArgs& a, cudaStream_t st);  // RemoveDivergence only
 int launch_z_solves(const StageArgs& a, cudaStream_t st);   // CN solve + RemoveDivergence
+int launch_fft_y_combos(const StageArgs& a, cudaStream_t st);   // 3D: mixout's 8 combinations -> rnl
 // TimeStepAdjoint's stage (sf_adjoint.cu): the direct state of the substep
 // into a.adir, then the adjoint x pass and the z solves; 2D
 int launch_stage_adjoint(StageArgs a, const float2* below, const float2* above, float frac, float2* adir,

@@ -1072,6 +1072,10 @@ static void launch_fft_y(const StageArgs& a, cudaStream_t st) {
     case 256: fy_launch<256>(a, st); break;
   }
 }
+int launch_fft_y_combos(const StageArgs& a, cudaStream_t st) {
+  launch_fft_y(a, st);
+  return 1;
+}
 
 // opt-in shared-memory limits of every kernel, set once per process before
 // any launch (and outside stream capture)

@@ -46,6 +46,7 @@ struct sf_solver {
   float2* tw = nullptr;
   float2* stage_ref = nullptr;   // one field in the reference layout
   float2* adir = nullptr;        // adjoint step: the direct state of the substep
+  float2* amix = nullptr;        // 3D adjoint step: 12 y-transformed fields
   std::vector<float> hRi;
   std::vector<double> zN, zfN;   // grid (for inspection)
   int cur = 0;                   // index of the current state buffer
@@ -78,7 +79,7 @@ static void free_all(sf_solver* s) {
   for (int l = 0; l < 2; l++)
     for (int p = 0; p < 2; p++)
       if (s->graph[l][p]) cudaGraphExecDestroy(s->graph[l][p]);
-  void* ptrs[] = {s->adir, s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
+  void* ptrs[] = {s->amix, s->adir, s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
                   s->fc, s->inv_den, s->kx, s->ky, s->Ri, s->Ubar, s->dBdz, s->bands, s->kxd, s->kyd,
                   s->red, s->tw, s->stage_ref};
   for (void* p : ptrs)
@@ -662,13 +663,14 @@ extern "C" int sf_velocity_maxima(sf_solver* s, int run, double* out3);
 int sf_step_adjoint(sf_solver* s, const void* below, const void* above) {
   if (!s || !below || !above) return fail(SF_EINVAL, "bad argument");
   const Geo& g = s->g;
-  if (g.dim3) return fail(SF_EINVAL, "the adjoint step is two-dimensional in this version");
   if (!s->adir) CK(cudaMalloc(&s->adir, sizeof(float2) * (size_t)4 * g.fblk * g.nrun));
+  if (g.dim3 && !s->amix) CK(cudaMalloc(&s->amix, sizeof(float2) * (size_t)12 * g.mblk * g.nrun));
   float frac = 0.f;
   int cur = s->cur;
   for (int k = 0; k < 3; k++) {
     StageArgs a = stage_args(s, k, cur, false);
     a.tlm = 0;
+    a.amix = s->amix;
     a.adj_invK = 0.5f;   // 1/K, K = 2 (IMEXRK.h:487)
     s->launches += launch_stage_adjoint(a, static_cast<const float2*>(below), static_cast<const float2*>(above), frac,
                                         s->adir, s->st);
