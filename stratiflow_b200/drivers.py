@@ -407,3 +407,59 @@ class LearnedPredictor:
         y = self.net.forward(self._inputs(pts[-2], pts[-1], ds)[None])[0]
         corr = self._unfeat(y[:, :self.nc].astype(np.float64) * self.scale["t"])
         return (sec_guess[0] + corr).astype(np.complex64), sec_guess[1]
+
+
+# ----------------------------------------------- adjoint optimisation step
+def solve_quadratic(a, b, c, positive=False):
+    """SolveQuadratic (Integration.cpp:3-22): a root of a x^2 + b x + c, 0 if
+    the roots are complex."""
+    disc = b * b - 4 * a * c
+    if disc < 0:
+        return 0.0
+    return (-b + np.sqrt(disc)) / (2 * a) if positive else (-b - np.sqrt(disc)) / (2 * a)
+
+
+def optimal_mixing_step(solver, x0, steps, epsilon):
+    """One update of the initial perturbation towards more mixing
+    (Adjoint.cpp:11-103): the adjoint of the mixing objective from a zero
+    final state back to t = 0 through `steps` fixed steps of run 0
+    (IMEXRK.AdjointEvolve), b of the adjoint divided by Ri, a step of size
+    epsilon along the gradient projected onto the sphere of the initial
+    energy (lambda from SolveQuadratic, epsilon halved while it has no real
+    root), then Rescale (StateVector.cpp:189-226) to that energy.
+    x0: kept-layout state [5][N3][plane]. Returns (new state, info)."""
+    from . import Vecs
+    assert solver.nrun == 1, "one run"
+    x0 = np.asarray(x0, dtype=np.complex64).reshape(solver.kept_shape[1:])
+    zero = np.zeros(solver.kept_shape, dtype=np.complex64)
+    adj = solver.AdjointEvolve(x0[None], zero, steps)[0].copy()
+    Ri = float(solver.Ri[0])
+    adj[3] /= Ri
+    V = Vecs(solver, 3)
+    V.set(0, x0)
+    V.set(1, adj)
+    udotu, udotv = V.dots(0, 2, V, 0, Ri)
+    vdotv = V.dots(1, 1, V, 1, Ri)[0]
+    lam = 0.0
+    while lam == 0.0:
+        lam = solve_quadratic(epsilon * udotu, 2 * epsilon * udotv - 2 * udotu, epsilon * vdotv - 2 * udotv)
+        if lam == 0.0:
+            epsilon /= 2
+    # deriv = adjoint + lambda x0; result = x0 - epsilon deriv (on u1..b)
+    V.copy(2, V, 1)
+    V.axpy(2, lam, V, 0)
+    residual = V.dots(2, 1, V, 2, Ri)[0]
+    V.lincomb(2, -epsilon, 1.0, V, 0)
+    # Rescale to the energy of x0: project, scale, project
+    energy = 0.5 * udotu
+    V.zero_pressure(2)
+    V.to_run(2, 0)
+    solver.Prepare()
+    V.from_run(2, 0)
+    e_before = 0.5 * V.dots(2, 1, V, 2, Ri)[0]
+    V.scale(2, np.sqrt(energy / e_before) if e_before != 0 else 0.0)
+    V.to_run(2, 0)
+    solver.Prepare()
+    out = solver.get_state_kept()[0]
+    return out, {"epsilon": epsilon, "lambda": lam, "residual": residual, "udotu": udotu, "udotv": udotv,
+                 "vdotv": vdotv, "bound_epsilon": -2 * udotu / udotv if udotv != 0 else None}

@@ -95,3 +95,61 @@ def test_adjoint_step_3d_matches_oracle():
     for k in ("u1", "u2", "u3", "b"):
         assert rel_l2(s.get_field(0, k), o.get_field(k)) < 1e-5, k
     assert rel_l2(s.get_field(0, "p"), o.get_field("p")) < 5e-4
+
+
+def test_optimal_mixing_step_matches_oracle():
+    """One update of Adjoint.cpp (adjoint from a zero final state, gradient
+    step on the energy sphere, Rescale) against the same arithmetic on the
+    FP64 oracle's forward and adjoint integrations (numpy for the update)."""
+    from stratiflow_b200 import drivers as D
+    from tests.test_vecs_drivers_gpu import _flow
+    cfg = CONFIGS["kh2d"]
+    x0d = make_ic(cfg, seed=551, amp=5e-2)
+    s = gpu_solver(cfg)
+    x0 = _kept(cfg, [x0d])[0]
+    new, info = D.optimal_mixing_step(s, x0, 3, 0.05)
+    # the oracle
+    o = make_oracle(cfg, 64)
+    o.set_state(x0d)
+    o.prepare()
+    snaps = [o.get_state()]
+    for _ in range(3):
+        o.step(1)
+        snaps.append(o.get_state())
+    zero = {k: np.zeros_like(v) for k, v in x0d.items()}
+    o.set_state(zero)
+    o.prepare()
+    for step in range(3):
+        o.step_adjoint(snaps[2 - step], snaps[3 - step])
+    adj = o.get_state()
+    adj["b"] = adj["b"] / cfg["Ri"]
+    flow = _flow(cfg)
+    tmp = gpu_solver(cfg)
+    def kept(st):
+        tmp.set_state(0, st)
+        return tmp.get_state_kept()[0].astype(np.complex128)
+    xk, vk = kept(x0d), kept(adj)
+    xk[4] = 0
+    vk[4] = 0
+    dot = lambda a, b: D.ext_dot(flow, (a, 0.0), (b, 0.0), cfg["Ri"])
+    uu, uv, vv = dot(xk, xk), dot(xk, vk), dot(vk, vk)
+    assert abs(info["udotv"] - uv) <= 1e-4 * np.sqrt(uu * vv)
+    eps = 0.05
+    lam = 0.0
+    while lam == 0.0:
+        lam = D.solve_quadratic(eps * uu, 2 * eps * uv - 2 * uu, eps * vv - 2 * uv)
+        if lam == 0.0:
+            eps /= 2
+    assert abs(info["lambda"] - lam) <= 1e-3 * abs(lam)
+    res = xk - eps * (vk + lam * xk)
+    # Rescale on the oracle: project, scale to the energy of x0, project
+    tmp.set_state_kept(res[None].astype(np.complex64))
+    tmp.Prepare()
+    r1 = tmp.get_state_kept()[0].astype(np.complex128)
+    r1[4] = 0
+    r1 *= np.sqrt(0.5 * uu / (0.5 * dot(r1, r1)))
+    tmp.set_state_kept(r1[None].astype(np.complex64))
+    tmp.Prepare()
+    want = tmp.get_state_kept()[0]
+    for f in (0, 2, 3):
+        assert rel_l2(new[f], want[f]) < 1e-4, f
