@@ -179,11 +179,11 @@ __device__ __forceinline__ void term_set(PTerm& T, int F, int Fm, float a0, floa
   T.Gs = Gs; T.Gp = Gp; T.b0 = b0; T.b1 = b1; T.b2 = b2;
 }
 
-// the terms of product p at slot s (level t); rows of the nodal fields
-// U1,U2,U3,B (`nr`) and of the frozen base (`br`: U1b+U_, U2b, U3b, Bb)
-template <bool LINEAR>
-__device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, int NS, const float* Ub,
-                                           const float* zc, PTerm& T0, PTerm& T1) {
+// the terms of product p of BuildRHSLinear (IMEXRK.cpp:212-257) at slot s
+// (level t); rows of the nodal fields U1,U2,U3,B (`nr`) and of the base
+// (`br`: U1b+U_, U2b, U3b, Bb)
+__device__ __forceinline__ void prod_terms_linear(int p, int s, int t, int N3, int N1, int NS, const float* zc,
+                                                  PTerm& T0, PTerm& T1) {
   // the base rows follow the nodal rows in shared memory (x_layout)
   auto nr = [&](int f, int ss) { return (f * NS + ss) * N1; };
   auto br = [&](int f, int ss) { return ((4 + f) * NS + ss) * N1; };
@@ -194,73 +194,119 @@ __device__ __forceinline__ void prod_terms(int p, int s, int t, int N3, int N1, 
   const float lof = lo ? 1.f : 0.f;
   const float tlo = lof * zc[ZC_TILDE_LO * N3 + t], tdi = lof * zc[ZC_TILDE_DI * N3 + t];
   const float hb = 0.5f * lof;
-  const float ub = Ub[t], ubm = lo ? Ub[t - 1] : 0.f;
   const int z = nr(0, s);   // any valid row for unused terms
   term_set(T1, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
-  if (!LINEAR) {
-    switch (p) {
-      // U1t*U1t enters only through ddx (IMEXRK.cpp:155-156); its x-independent
-      // U_^2 part lies in the kx = 0 mode, which ddx multiplies by zero, so it
-      // is left out of the product to keep the FP32 rounding small
-      case P_S1: term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 2.f * ub); break;
-      case P_SB1: term_set(T0, nr(0, s), z, 1.f, 0.f, ub, nr(3, s), z, 1.f, 0.f, 0.f); break;
-      case P_P3: term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, tlo * ubm + tdi * ub, nr(2, s), z, lof, 0.f, 0.f); break;
-      case P_Q1: term_set(T0, nr(0, s), nr(0, sm), hb, hb, hb * ubm + hb * ub, nr(2, s), z, lof, 0.f, 0.f); break;
-      case P_QB: term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
-      case P_P4: term_set(T0, nr(2, s), nr(2, sp), 0.5f, 0.5f * top, 0.f, nr(2, s), nr(2, sp), 0.5f, 0.5f * top, 0.f); break;
-      case P_S12: term_set(T0, nr(0, s), z, 1.f, 0.f, ub, nr(1, s), z, 1.f, 0.f, 0.f); break;
-      case P_S22: term_set(T0, nr(1, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f); break;
-      case P_SB2: term_set(T0, nr(1, s), z, 1.f, 0.f, 0.f, nr(3, s), z, 1.f, 0.f, 0.f); break;
-      case P_Q2: term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
-      case P_P3Y: term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f); break;
-      default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
-    }
-  } else {
-    switch (p) {
-      case P_S1: term_set(T0, nr(0, s), z, 2.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f); break;
-      case P_SB1:
-        term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f);
-        term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 0.f);
-        break;
-      case P_P3:
-        term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
-        term_set(T1, br(0, s), br(0, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-        break;
-      case P_Q1:
-        term_set(T0, nr(0, s), nr(0, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-        term_set(T1, br(0, s), br(0, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-        break;
-      case P_QB:
-        term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-        term_set(T1, br(3, s), br(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-        break;
-      case P_P4:   // 2 Dir(U3) Dir(U3b)
-        term_set(T0, nr(2, s), nr(2, sp), 1.f, top, 0.f, br(2, s), br(2, sp), 0.5f, 0.5f * top, 0.f);
-        break;
-      case P_S12:
-        term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
-        term_set(T1, br(0, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
-        break;
-      case P_S22: term_set(T0, nr(1, s), z, 2.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f); break;
-      case P_SB2:
-        term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
-        term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
-        break;
-      case P_Q2:
-        term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-        term_set(T1, br(1, s), br(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-        break;
-      case P_P3Y:
-        term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
-        term_set(T1, br(1, s), br(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-        break;
-      default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
-    }
+  switch (p) {
+    case P_S1: term_set(T0, nr(0, s), z, 2.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f); break;
+    case P_SB1:
+      term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f);
+      term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 0.f);
+      break;
+    case P_P3:
+      term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
+      term_set(T1, br(0, s), br(0, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+      break;
+    case P_Q1:
+      term_set(T0, nr(0, s), nr(0, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+      term_set(T1, br(0, s), br(0, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+      break;
+    case P_QB:
+      term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+      term_set(T1, br(3, s), br(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+      break;
+    case P_P4:   // 2 Dir(U3) Dir(U3b)
+      term_set(T0, nr(2, s), nr(2, sp), 1.f, top, 0.f, br(2, s), br(2, sp), 0.5f, 0.5f * top, 0.f);
+      break;
+    case P_S12:
+      term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
+      term_set(T1, br(0, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
+      break;
+    case P_S22: term_set(T0, nr(1, s), z, 2.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f); break;
+    case P_SB2:
+      term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
+      term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
+      break;
+    case P_Q2:
+      term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
+      term_set(T1, br(1, s), br(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+      break;
+    case P_P3Y:
+      term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
+      term_set(T1, br(1, s), br(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
+      break;
+    default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
   }
 }
 
 __device__ __forceinline__ float term_eval(const float* rows, const PTerm& T, int x) {
   return (T.a0 * rows[T.F + x] + T.a1 * rows[T.Fm + x] + T.a2) * (T.b0 * rows[T.Gs + x] + T.b1 * rows[T.Gp + x] + T.b2);
+}
+
+// ---- BuildRHS products by pair (the nonlinear x pass) ----
+// Each forward transform carries two real products; a pair kind fixes which
+// two, so the rows each lane reads and the arithmetic are compile-time
+// constants and the two products of a pair share their loads. Products at
+// slot i + 1 of a slab (i < S): (S1, SB1), (P3, P4), (S12, S22), (SB2, P3Y);
+// the Q products at slot i + 2: (Q1, QB) and (Q2 at i + 2, Q2 at i + 3); the
+// slab's first halo rows, (Q1, QB) at slot 1 and (P4 at slot 0, Q2 at slot 1),
+// when no slab below handed them over.
+enum PairKind { K_SSB1, K_P34, K_S122, K_SB2P, K_QQB, K_Q2Q2, K_HALO };
+
+struct HalfC {  // one product at one slot: its rows and coefficients
+  int s, sm, sp;
+  float ub, ubm, tlo, tdi, hb, lof, top;
+  bool live;
+};
+
+__device__ __forceinline__ HalfC half_coeffs(int s, int j0, int N3, const float* Ub, const float* zc) {
+  HalfC c;
+  const int t = j0 - 1 + s;
+  c.live = t >= 0 && t < N3;
+  const int tc = c.live ? t : 0;
+  const bool lo = c.live && (t >= 1) && (s >= 1);
+  c.s = s;
+  c.sm = lo ? s - 1 : s;
+  c.top = (t <= N3 - 2) ? 1.f : 0.f;
+  c.sp = (t <= N3 - 2) ? s + 1 : s;
+  c.lof = lo ? 1.f : 0.f;
+  c.tlo = c.lof * zc[ZC_TILDE_LO * N3 + tc];
+  c.tdi = c.lof * zc[ZC_TILDE_DI * N3 + tc];
+  c.hb = 0.5f * c.lof;
+  c.ub = Ub[tc];
+  c.ubm = lo ? Ub[tc - 1] : 0.f;
+  return c;
+}
+
+// product P of BuildRHS at point n (IMEXRK.cpp:155-192; the U1t*U1t product
+// leaves out its x-independent U_^2 part, which ddx multiplies by zero)
+template <int P, int N1>
+__device__ __forceinline__ float prod_at(const float* nod, int NS, const HalfC& c, int n) {
+  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * N1 + n]; };
+  float v;
+  if constexpr (P == P_S1) { const float a = u(0, c.s); v = a * (a + 2.f * c.ub); }
+  else if constexpr (P == P_SB1) v = (u(0, c.s) + c.ub) * u(3, c.s);
+  else if constexpr (P == P_P3)
+    v = (c.tdi * u(0, c.s) + c.tlo * u(0, c.sm) + (c.tlo * c.ubm + c.tdi * c.ub)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_Q1)
+    v = (c.hb * u(0, c.s) + c.hb * u(0, c.sm) + (c.hb * c.ubm + c.hb * c.ub)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_QB) v = (c.hb * u(3, c.s) + c.hb * u(3, c.sm)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_P4) { const float d = 0.5f * u(2, c.s) + 0.5f * c.top * u(2, c.sp); v = d * d; }
+  else if constexpr (P == P_S12) v = (u(0, c.s) + c.ub) * u(1, c.s);
+  else if constexpr (P == P_S22) { const float a = u(1, c.s); v = a * a; }
+  else if constexpr (P == P_SB2) v = u(1, c.s) * u(3, c.s);
+  else if constexpr (P == P_Q2) v = (c.hb * u(1, c.s) + c.hb * u(1, c.sm)) * (c.lof * u(2, c.s));
+  else v = (c.tdi * u(1, c.s) + c.tlo * u(1, c.sm)) * (c.lof * u(2, c.s));   // P_P3Y
+  return c.live ? v : 0.f;
+}
+
+template <int P0, int P1, int N1, int E, int G>
+__device__ __forceinline__ void pair_eval(float2 (&x)[E], const float* nod, int NS, const HalfC& c0, const HalfC& c1,
+                                          bool two, int l) {
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int n = l + G * e;
+    x[e] = make_float2(prod_at<P0, N1>(nod, NS, c0, n), two ? prod_at<P1, N1>(nod, NS, c1, n) : 0.f);
+  }
 }
 
 __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
@@ -391,59 +437,115 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
 
   // ---- phase B/C: nodal products, forward transforms in pairs (ToModal) ----
   const int nprod = L.nprod;
-  int ncar = 0;
-  for (int p = 0; p < nprod; p++) ncar += carried(p) ? 1 : 0;
-  const int nrows = L.nrows - (it > 0 ? ncar : 0);
-  const int ntB = (nrows + 1) / 2;
   const float sc = 0.5f * g.inv_n12;
-  for (int base = 0; base < ntB; base += NGB) {
-    const int task = base + gid;
-    int pp[2], ss[2], row[2];
-    bool live[2];
-    PTerm T[2][2];
+  if constexpr (!LINEAR) {
+    const int NT = g.dim3 ? 5 : 3;   // pair kinds at every output level
+    const int nmain = NT * S, nq2 = g.dim3 ? (S + 1) / 2 : 0, ntB = nmain + nq2 + (it == 0 ? 2 : 0);
+    for (int base = 0; base < ntB; base += NGB) {
+      const int task = base + gid;
+      int kind = -1, i = 0;
+      if (task < nmain) {
+        const int q = task / S;
+        kind = q < 2 ? q : (g.dim3 ? q : K_QQB);   // 2D: (S1, SB1), (P3, P4), (Q1, QB)
+        i = task - q * S;
+      } else if (task < nmain + nq2) {
+        kind = K_Q2Q2;
+        i = 2 * (task - nmain);
+      } else if (task < ntB) {
+        kind = task == nmain + nq2 ? K_QQB : K_HALO;
+        i = -1;
+      }
+      int s0 = i + 1, s1 = i + 1, p0 = -1, p1 = -1;
+      switch (kind) {
+        case K_SSB1: p0 = P_S1; p1 = P_SB1; break;
+        case K_P34: p0 = P_P3; p1 = P_P4; break;
+        case K_S122: p0 = P_S12; p1 = P_S22; break;
+        case K_SB2P: p0 = P_SB2; p1 = P_P3Y; break;
+        case K_QQB: p0 = P_Q1; p1 = P_QB; s0 = s1 = i + 2; break;
+        case K_Q2Q2: p0 = P_Q2; p1 = i + 1 < S ? P_Q2 : -1; s0 = i + 2; s1 = i + 3; break;
+        case K_HALO: p0 = P_P4; p1 = g.dim3 ? P_Q2 : -1; s0 = 0; s1 = 1; break;
+        default: break;
+      }
+      const HalfC c0 = half_coeffs(s0, j0, N3, Ub, zc), c1 = half_coeffs(s1, j0, N3, Ub, zc);
+      const bool two = p1 >= 0;
+      float2 x[E];
+      switch (kind) {
+        case K_SSB1: pair_eval<P_S1, P_SB1, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
+        case K_P34: pair_eval<P_P3, P_P4, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
+        case K_S122: pair_eval<P_S12, P_S22, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
+        case K_SB2P: pair_eval<P_SB2, P_P3Y, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
+        case K_QQB: pair_eval<P_Q1, P_QB, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
+        case K_Q2Q2: pair_eval<P_Q2, P_Q2, N1, E, G>(x, nod, NS, c0, c1, two, l); break;
+        case K_HALO: pair_eval<P_P4, P_Q2, N1, E, G>(x, nod, NS, c0, c1, two, l); break;
+        default:
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-      int r = 2 * task + h;
-      pp[h] = -1; ss[h] = 0; live[h] = false; row[h] = r;
-      if (task < ntB && r < nrows) {
-        for (int p = 0; p < nprod; p++) {
-          int f0, c; prod_slots(p, S, f0, c);
-          const int skip = (it > 0 && carried(p)) ? 1 : 0;
-          if (r < c - skip) { pp[h] = p; ss[h] = f0 + skip + r; break; }
-          r -= c - skip;
+          for (int e = 0; e < E; e++) x[e] = make_float2(0.f, 0.f);
+      }
+      reg_fft<N1, false>(x, buf, a.tw, l);
+#pragma unroll
+      for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
+      __syncwarp();
+      if (p0 >= 0) {
+        float2* h0 = hat + (size_t)hat_row(p0, s0, S) * K1;
+        float2* h1 = hat + (size_t)hat_row(two ? p1 : p0, s1, S) * K1;
+        for (int k = l; k < K1; k += G) {
+          const float2 zk = buf[k];
+          const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
+          h0[k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);          // (Zk + conj Z_{N-k}) / 2
+          if (two) h1[k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);  // (Zk - conj Z_{N-k}) / (2i)
         }
-        if (pp[h] >= 0) row[h] = hat_row(pp[h], ss[h], S);
-        const int t = j0 - 1 + ss[h];
-        live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
       }
-      prod_terms<LINEAR>(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, Ub, zc, T[h][0],
-                         T[h][1]);
+      __syncwarp();
     }
-    float2 x[E];
+  } else {
+    int ncar = 0;
+    for (int p = 0; p < nprod; p++) ncar += carried(p) ? 1 : 0;
+    const int nrows = L.nrows - (it > 0 ? ncar : 0);
+    const int ntB = (nrows + 1) / 2;
+    for (int base = 0; base < ntB; base += NGB) {
+      const int task = base + gid;
+      int pp[2], ss[2], row[2];
+      bool live[2];
+      PTerm T[2][2];
 #pragma unroll
-    for (int e = 0; e < E; e++) {
-      const int n = l + G * e;
-      float v0 = term_eval(nod, T[0][0], n), v1 = term_eval(nod, T[1][0], n);
-      if (LINEAR) {
-        v0 += term_eval(nod, T[0][1], n);
-        v1 += term_eval(nod, T[1][1], n);
+      for (int h = 0; h < 2; h++) {
+        int r = 2 * task + h;
+        pp[h] = -1; ss[h] = 0; live[h] = false; row[h] = r;
+        if (task < ntB && r < nrows) {
+          for (int p = 0; p < nprod; p++) {
+            int f0, c; prod_slots(p, S, f0, c);
+            const int skip = (it > 0 && carried(p)) ? 1 : 0;
+            if (r < c - skip) { pp[h] = p; ss[h] = f0 + skip + r; break; }
+            r -= c - skip;
+          }
+          if (pp[h] >= 0) row[h] = hat_row(pp[h], ss[h], S);
+          const int t = j0 - 1 + ss[h];
+          live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
+        }
+        prod_terms_linear(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, zc, T[h][0], T[h][1]);
       }
-      x[e] = make_float2(v0, v1);
-    }
-    reg_fft<N1, false>(x, buf, a.tw, l);
-    // natural order in the group's buffer, then split the two real transforms
+      float2 x[E];
 #pragma unroll
-    for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
-    __syncwarp();
-    for (int k = l; k < K1; k += G) {
-      const float2 zk = buf[k];
-      const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
-      if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
-        hat[(size_t)row[0] * K1 + k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);
-      if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
-        hat[(size_t)row[1] * K1 + k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);
+      for (int e = 0; e < E; e++) {
+        const int n = l + G * e;
+        x[e] = make_float2(term_eval(nod, T[0][0], n) + term_eval(nod, T[0][1], n),
+                           term_eval(nod, T[1][0], n) + term_eval(nod, T[1][1], n));
+      }
+      reg_fft<N1, false>(x, buf, a.tw, l);
+      // natural order in the group's buffer, then split the two real transforms
+#pragma unroll
+      for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
+      __syncwarp();
+      for (int k = l; k < K1; k += G) {
+        const float2 zk = buf[k];
+        const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
+        if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
+          hat[(size_t)row[0] * K1 + k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);
+        if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
+          hat[(size_t)row[1] * K1 + k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);
+      }
+      __syncwarp();
     }
-    __syncwarp();
   }
   __syncthreads();
 
