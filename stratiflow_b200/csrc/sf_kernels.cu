@@ -141,21 +141,28 @@ __host__ __device__ __forceinline__ bool carried(int p) {
 
 struct XLayout {  // shared-memory carve-up of k_xpass
   int nprod, nrows;
-  size_t hat_off, buf_off, nod_off, base_off, carry_off, bytes;
+  size_t hat_off, stage_off, buf_off, nod_off, base_off, carry_off, bytes;
 };
 
 __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int linear, int bufstride, int ngroups,
-                                            int tlm = 0) {
+                                            int tlm, int prefetch) {
   XLayout L;
   L.nprod = dim3 ? P_COUNT : 6;
   L.nrows = prod_rows(L.nprod, S);
   size_t off = 0;
-  // transformed products, one row of K1 per (product, slot); before phase B
-  // the same bytes stage the input rows of phase A (4 x (S+2) x K1, twice
-  // that when the base rows of a tangent-linear batch come along)
+  // transformed products, one row of K1 per (product, slot), and the staged
+  // input rows of phase A (4 x (S+2) x K1, twice that when the base rows of
+  // a tangent-linear batch come along): their own bytes when a block loads
+  // the next slab's rows during this slab's work, else the same bytes
   size_t hat = sizeof(float2) * (size_t)L.nrows * K1,
          stage = sizeof(float2) * (size_t)(tlm ? 8 : 4) * (S + 2) * K1;
-  L.hat_off = off;  off += (hat > stage ? hat : stage);
+  L.hat_off = off;
+  if (prefetch) {
+    off += hat;
+    L.stage_off = off; off += stage;
+  } else {
+    L.stage_off = off; off += (hat > stage ? hat : stage);
+  }
   L.buf_off = off;  off += sizeof(float2) * (size_t)ngroups * bufstride;
   L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
   L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
@@ -329,9 +336,9 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   const Geo g = a.g;
   extern __shared__ __align__(16) unsigned char xsm[];
   const int tlm = LINEAR ? a.tlm : 0;   // base rows from a live run of this batch
-  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB, tlm);
+  const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB, tlm, iters > 1);
   float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
-  float2* stg = hat;                                           // phase A input rows [4 or 8][S+2][K1]
+  float2* stg = reinterpret_cast<float2*>(xsm + L.stage_off);  // phase A input rows [4 or 8][S+2][K1]
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
   const int K1 = g.K1, N3 = g.N3;
@@ -346,26 +353,32 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   const int nf = tlm ? 8 : 4;   // own u1,u2,u3,b (and the base run's)
   float2* carry = reinterpret_cast<float2*>(xsm + L.carry_off);   // [4][K1]: Q1, QB, Q2, P4
 
+  // stage the input rows u1, u2, u3, b (and the base run's) at slots s0..S+1
+  // (levels jj0-1+s0 .. jj0+S) with asynchronous copies, one warp per row
+  auto stage_rows = [&](int jj0, int s0) {
+    const int NSn = NS - s0, nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int row = threadIdx.x >> 5; row < nf * NSn; row += nw) {
+      const int fb = row / NSn, s = s0 + row - fb * NSn;
+      const int f = fb & 3, rr = fb < 4 ? run : brun;
+      const int t = jj0 - 1 + s;
+      float2* d = stg + ((size_t)fb * NS + s) * K1;
+      if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
+        for (int k = lane; k < K1; k += 32) d[k] = make_float2(0.f, 0.f);
+      } else {
+        const float2* src = g.dim3 ? a.mixin + (((size_t)(rr * 4 + f) * N3 + t) * g.N2 + y) * K1
+                                   : a.S + ((size_t)(rr * 5 + f) * N3 + t) * g.Pp;
+        for (int k = lane; k < K1; k += 32) cp_async8(d + k, src + k);
+      }
+    }
+  };
+  stage_rows(blockIdx.x * iters * S, 0);
+
   for (int it = 0; it < iters; it++) {
   const int j0 = (blockIdx.x * iters + it) * S;
   if (j0 >= N3) break;
   const int s0 = it == 0 ? 0 : 2;   // nodal slots 0, 1 come from the slab below
   const int NSn = NS - s0;
 
-  // ---- stage the input rows (u1,u2,u3,b at levels j0-1+s0 .. j0+S) ----
-  for (int i = threadIdx.x; i < nf * NSn * K1; i += blockDim.x) {
-    const int fb = i / (NSn * K1), r = i - fb * NSn * K1, s = s0 + r / K1, k = r - (s - s0) * K1;
-    const int f = fb & 3, rr = fb < 4 ? run : brun;
-    const int t = j0 - 1 + s;
-    float2* d = stg + ((size_t)fb * NS + s) * K1 + k;
-    if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
-      *d = make_float2(0.f, 0.f);
-    } else if (g.dim3) {
-      cp_async8(d, a.mixin + (((size_t)(rr * 4 + f) * N3 + t) * g.N2 + y) * K1 + k);
-    } else {
-      cp_async8(d, a.S + ((size_t)(rr * 5 + f) * N3 + t) * g.Pp + k);
-    }
-  }
   if (LINEAR && !tlm) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
     for (int i = threadIdx.x; i < 4 * NS * N1; i += blockDim.x) {
       int f = i / (NS * N1), r = i - f * NS * N1, s = r / N1, x = r - s * N1;
@@ -427,7 +440,10 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   }
   __syncthreads();
 
-  // rows carried over from the slab below (the staging area above overlaid them)
+  // the next slab's input rows load while this slab's products are formed
+  if (it + 1 < iters && j0 + S < N3) stage_rows(j0 + S, 2);
+
+  // rows carried over from the slab below
   if (it > 0)
     for (int i = threadIdx.x; i < 4 * K1; i += blockDim.x) {
       const int q = i / K1, k = i - q * K1;
@@ -488,7 +504,10 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
       if (p0 >= 0) {
         float2* h0 = hat + (size_t)hat_row(p0, s0, S) * K1;
         float2* h1 = hat + (size_t)hat_row(two ? p1 : p0, s1, S) * K1;
-        for (int k = l; k < K1; k += G) {
+#pragma unroll
+        for (int q = 0; q < (N1 / 3 + G - 1) / G; q++) {   // K1 <= N1 / 3
+          const int k = l + q * G;
+          if (k >= K1) break;
           const float2 zk = buf[k];
           const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
           h0[k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);          // (Zk + conj Z_{N-k}) / 2
@@ -551,8 +570,11 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
 
   // ---- phase D: z stencils of the products and x derivatives ----
   auto H = [&](int p, int s, int k) -> float2 { return hat[(size_t)hat_row(p, s, S) * K1 + k]; };
+  const float inv_k1 = 1.f / K1;
   for (int i = threadIdx.x; i < S * K1; i += blockDim.x) {
-    const int si = i / K1, k = i - si * K1;
+    // i / K1 through the reciprocal: (i + 1/2) / K1 stays at least 1 / (2 K1)
+    // from an integer, far beyond the rounding of one product at i < 2^16
+    const int si = (int)(((float)i + 0.5f) * inv_k1), k = i - si * K1;
     const int t = j0 + si, s = si + 1;
     if (t >= N3) continue;
     const float kxv = a.kx[k];
@@ -1090,14 +1112,14 @@ static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
     int t = ((groups * G + 31) / 32) * 32;
     return t < 64 ? 64 : (t > kXMaxThreads ? kXMaxThreads : t);
   };
-  auto bytes = [&](int S) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, threads(S) / G, tlm).bytes; };
+  auto bytes = [&](int S, int pre) { return x_layout(S, N1, g.K1, g.dim3, LIN, BUF, threads(S) / G, tlm, pre).bytes; };
   (void)nprod;
   // largest slab whose shared memory lets two blocks share an SM, then
   // smaller slabs while the grid would leave SMs idle
   const int cand[] = {8, 6, 4, 3, 2};
   int S = 2;
   for (int c : cand)
-    if (bytes(c) <= 112 * 1024) { S = c; break; }
+    if (bytes(c, g.dim3) <= 112 * 1024) { S = c; break; }
   if (g.dim3 && S > 4) S = 4;
   for (int i = 0; i < 5; i++) {
     if (cand[i] >= S) continue;
@@ -1113,8 +1135,9 @@ static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
          (long long)cdiv(g.N3, S * (iters + 1)) * g.N2 * nruns >= 4 * 148)
     iters++;
   if (a.xslabs > 0) iters = std::min<int>(a.xslabs, (int)cdiv(g.N3, S));
+  if (iters > 1 && bytes(S, 1) > 227 * 1024) iters = 1;   // no room for the prefetch buffer
   dim3 grid(cdiv(g.N3, S * iters), g.N2, nruns);
-  k_xpass<N1, LIN><<<grid, threads(S), bytes(S), st>>>(a, S, iters);
+  k_xpass<N1, LIN><<<grid, threads(S), bytes(S, iters > 1), st>>>(a, S, iters);
 }
 
 static void launch_xpass_runs(const StageArgs& a, bool L, int nruns, cudaStream_t st) {
