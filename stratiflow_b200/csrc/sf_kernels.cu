@@ -644,7 +644,9 @@ constexpr int kZU = 8;   // levels of every input loaded ahead per thread
 // replays its levels from the right incoming value. be_j and D_j stay in
 // shared memory ([N3][32] floats per block). The result equals the sequential
 // sweep up to rounding.
-constexpr int kZU2 = 4;   // levels loaded ahead in the chunked z kernels
+constexpr int kZU2 = 4;   // levels of every input loaded ahead in the chunked z kernels' first sweep
+constexpr int kZI = 16;   // levels of inverse pivots loaded ahead in their later sweeps
+constexpr int kZP = 4;    // levels of the fields loaded ahead in the projection's last sweep
 
 template <int ZW>
 __device__ __forceinline__ void zscan_up(float* sA, float* sB, float* sIn, int w, int lane, float A, float B) {
@@ -675,12 +677,13 @@ __device__ __forceinline__ void zscan_down(float* sA, float* sB, float* sIn, int
   __syncthreads();
 }
 
-// the inverse pivots of levels j0, j0 + step, ... (kZU2 of them, those in
+// the inverse pivots of levels j0, j0 + step, ... (K of them, those in
 // [lo, hi)) loaded ahead of their use in the serial sweeps
-__device__ __forceinline__ void load_iden(float (&bi)[kZU2], const float* __restrict__ iden, int Pp, int j0, int step,
+template <int K>
+__device__ __forceinline__ void load_iden(float (&bi)[K], const float* __restrict__ iden, int Pp, int j0, int step,
                                           int lo, int hi) {
 #pragma unroll
-  for (int i = 0; i < kZU2; i++) {
+  for (int i = 0; i < K; i++) {
     const int j = j0 + step * i;
     bi[i] = (j >= lo && j < hi) ? iden[(size_t)j * Pp] : 0.f;
   }
@@ -812,11 +815,11 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   float D = sIn[w * 32 + lane];
   A = 1.f;
   B = 0.f;
-  for (int j0 = js; j0 < je; j0 += kZU2) {
-    float bi[kZU2];
+  for (int j0 = js; j0 < je; j0 += kZI) {
+    float bi[kZI];
     load_iden(bi, iden, Pp, j0, 1, js, je);
 #pragma unroll
-    for (int i = 0; i < kZU2; i++) {
+    for (int i = 0; i < kZI; i++) {
       const int j = j0 + i;
       if (j >= je) break;
       const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
@@ -830,11 +833,11 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   zscan_down<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- backward, pass 2: the solution ----
   float x = sIn[w * 32 + lane];
-  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
-    float bi[kZU2];
+  for (int j0 = je - 1; j0 >= js; j0 -= kZI) {
+    float bi[kZI];
     load_iden(bi, iden, Pp, j0, -1, js, je);
 #pragma unroll
-    for (int i = 0; i < kZU2; i++) {
+    for (int i = 0; i < kZI; i++) {
       const int j = j0 - i;
       if (j < js) break;
       const float Cj = fc[j] * bi[i];
@@ -926,11 +929,11 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
   float D = sIn[w * 32 + lane];
   A = 1.f;
   B = 0.f;
-  for (int j0 = js; j0 < je; j0 += kZU2) {
-    float bi[kZU2];
+  for (int j0 = js; j0 < je; j0 += kZI) {
+    float bi[kZI];
     load_iden(bi, iden, Pp, j0, 1, js, je);
 #pragma unroll
-    for (int i = 0; i < kZU2; i++) {
+    for (int i = 0; i < kZI; i++) {
       const int j = j0 + i;
       if (j >= je) break;
       const float al = (j == 0) ? 0.f : -a_[j] * bi[i];
@@ -944,26 +947,32 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
   zscan_down<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- backward, pass 2: q_j, projection, p ----
   float qn = sIn[w * 32 + lane];   // q at level je (0 above the top)
-  for (int j0 = je - 1; j0 >= js; j0 -= kZU2) {
-    float bi[kZU2], pv[kZU2];
+  // every row of u1, u2, u3, p is written once, by the step of one level,
+  // so the loads of a batch may all go ahead of its stores
+  for (int j0 = je - 1; j0 >= js; j0 -= kZP) {
+    float bi[kZP], pv[kZP], v1[kZP], v2[kZP], v3[kZP];
     load_iden(bi, iden, Pp, j0, -1, js, je);
 #pragma unroll
-    for (int i = 0; i < kZU2; i++) {
-      const int j = j0 - i;
-      pv[i] = (j >= js && act) ? ps[j * S2] : 0.f;
+    for (int i = 0; i < kZP; i++) {
+      const int j = j0 - i, jj = j + 1;
+      const bool in = j >= js && act;
+      pv[i] = in ? ps[j * S2] : 0.f;
+      v1[i] = in ? u1c[j * S2] : 0.f;
+      v2[i] = (in && g.dim3) ? u2c[j * S2] : 0.f;
+      v3[i] = (in && jj >= 2 && jj <= N3 - 1) ? u3[jj * S2] : 0.f;
     }
 #pragma unroll
-    for (int i = 0; i < kZU2; i++) {
+    for (int i = 0; i < kZP; i++) {
       const int j = j0 - i;
       if (j < js) break;
       const float qj = sD[j * 32 + lane] - Cof(j, bi[i]) * qn;
       const float qo = __shfl_xor_sync(0xffffffffu, qj, 1);
       if (act) {
-        u1c[j * S2] -= sc * kxv * qo;
-        if (g.dim3) u2c[j * S2] -= sc * kyv * qo;
+        u1c[j * S2] = v1[i] - sc * kxv * qo;
+        if (g.dim3) u2c[j * S2] = v2[i] - sc * kyv * qo;
         pd[j * S2] = pv[i] + pm * qj;
         const int jj = j + 1;   // u3_{j+1} -= ddz(q)_{j+1}, rows 2..N-1
-        if (jj >= 2 && jj <= N3 - 1) u3[jj * S2] -= dnd_lo[jj] * qj + dnd_di[jj] * qn;
+        if (jj >= 2 && jj <= N3 - 1) u3[jj * S2] = v3[i] - (dnd_lo[jj] * qj + dnd_di[jj] * qn);
       }
       qn = qj;
     }
