@@ -689,10 +689,11 @@ __device__ __forceinline__ void load_iden(float (&bi)[K], const float* __restric
   }
 }
 
-// k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
-// FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
-template <int ZW>
-__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(StageArgs a) {
+// the body of k_z_cn_chunked for field f of family FAM (0: u1 and u2,
+// 1: u3, Dirichlet; 2: b), so that each family's loads and terms are fixed
+// at compile time
+template <int ZW, int FAM>
+__device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
   const Geo g = a.g;
   extern __shared__ float zsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -700,8 +701,6 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   const bool act = m0 < g.P;
   const int m = act ? m0 : 0;
   const int run = blockIdx.z;
-  const int fi = blockIdx.y;
-  const int f = g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
   const int N3 = g.N3, Pp = g.Pp;
   const int chunk = (N3 + ZW - 1) / ZW;
   const int js = min(N3, w * chunk), je = min(N3, js + chunk);
@@ -713,9 +712,8 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   const float kxv = a.kx[j1], kyv = a.ky[q];
   const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
   const float sc = c == 0 ? -1.f : 1.f;   // (i k z)_c = sc * k * z_{1-c}
-  const bool dir = (f == 2);
-  const int fam = (f == 3) ? 1 : (dir ? 2 : 0);
-  const int fs = fam * 3 + a.stage;
+  constexpr bool dir = (FAM == 1);
+  const int fs = (FAM == 2 ? 1 : (dir ? 2 : 0)) * 3 + a.stage;   // factor sets: velocity, buoyancy, u3
   const float* __restrict__ fa = a.fa + (size_t)fs * N3;
   const float* __restrict__ fc = a.fc + (size_t)fs * N3;
   const float* __restrict__ iden = a.inv_den + (size_t)fs * N3 * Pp + m;
@@ -727,7 +725,7 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   const float* __restrict__ dnd_di = zc + ZC_DND_DI * N3;
   const float* __restrict__ full_lo = zc + ZC_FULL_LO * N3;
   const float* __restrict__ full_di = zc + ZC_FULL_DI * N3;
-  const float cco = (f == 3) ? a.cb : a.cv;
+  const float cco = (FAM == 2) ? a.cb : a.cv;
   const float Ri = a.Ri[run];
   const float* __restrict__ dB = a.dBdz + (size_t)run * N3;
   const bool zmode = (m == 0);   // the (0,0) mode: no buoyancy force (IMEXRK.cpp:141-143)
@@ -747,9 +745,9 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
   // ---- forward, pass 1: right-hand side, be_j, chunk map ----
   float um = js >= 1 && js < N3 ? uc[(js - 1) * S2] : 0.f;
   float u0 = js < N3 ? uc[js * S2] : 0.f;
-  float pm1 = (f == 2 && js >= 1 && js < N3) ? pc[(js - 1) * S2] : 0.f;
-  float bm1 = (f == 2 && js >= 1 && js < N3) ? bc[(js - 1) * S2] : 0.f;
-  float w0 = (f == 3 && js < N3) ? wc[js * S2] : 0.f;
+  float pm1 = (FAM == 1 && js >= 1 && js < N3) ? pc[(js - 1) * S2] : 0.f;
+  float bm1 = (FAM == 1 && js >= 1 && js < N3) ? bc[(js - 1) * S2] : 0.f;
+  float w0 = (FAM == 2 && js < N3) ? wc[js * S2] : 0.f;
   float A = 1.f, B = 0.f;
   for (int j0 = js; j0 < je; j0 += kZU2) {
     float bu[kZU2], br[kZU2], bo[kZU2], bp[kZU2], bx[kZU2], bi[kZU2];
@@ -763,12 +761,12 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
       bi[i] = in ? iden[(size_t)j * Pp] : 0.f;
       bp[i] = 0.f;
       bx[i] = 0.f;
-      if (f <= 1) bp[i] = in ? po[j * S2] : 0.f;
-      if (f == 2) {
+      if (FAM == 0) bp[i] = in ? po[j * S2] : 0.f;
+      if (FAM == 1) {
         bp[i] = in ? pc[j * S2] : 0.f;
         bx[i] = in ? bc[j * S2] : 0.f;
       }
-      if (f == 3) bx[i] = nx ? wc[(j + 1) * S2] : 0.f;
+      if (FAM == 2) bx[i] = nx ? wc[(j + 1) * S2] : 0.f;
     }
 #pragma unroll
     for (int i = 0; i < kZU2; i++) {
@@ -777,9 +775,9 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
       const float up = bu[i];
       float rt = br[i];
       float gp = 0.f;
-      if (f <= 1) {
+      if (FAM == 0) {
         gp = sc * kgrad * bp[i];   // (i k p)_c
-      } else if (f == 2) {
+      } else if (FAM == 1) {
         if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
         pm1 = bp[i];
         if (j >= 1 && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
@@ -845,6 +843,20 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(Stage
       if (act) out[j * S2] = x;
     }
   }
+}
+
+// k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
+// FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
+template <int ZW>
+__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(StageArgs a) {
+  const int fi = blockIdx.y;
+  const int f = a.g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
+  if (f <= 1)
+    z_cn_body<ZW, 0>(a, f);
+  else if (f == 2)
+    z_cn_body<ZW, 1>(a, f);
+  else
+    z_cn_body<ZW, 2>(a, f);
 }
 
 // RemoveDivergence with the chunked solve, for 16 modes per block: the
