@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   float2* stg = reinterpret_cast<float2*>(xsm + L.stage_off);  // phase A input rows [4 or 8][S+2][K1]
   float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
   float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
-  const int K1 = g.K1, N3 = g.N3;
+  constexpr int K1 = N1 / 3;   // kept x modes (the solver's K1), a compile-time constant here
+  const int N3 = g.N3;
   const int y = blockIdx.y;
   const int run = blockIdx.z + a.run_offset;
   const int brun = tlm ? (run - tlm) % tlm : run;   // run that holds the base state
@@ -505,7 +506,7 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
         float2* h0 = hat + (size_t)hat_row(p0, s0, S) * K1;
         float2* h1 = hat + (size_t)hat_row(two ? p1 : p0, s1, S) * K1;
 #pragma unroll
-        for (int q = 0; q < (N1 / 3 + G - 1) / G; q++) {   // K1 <= N1 / 3
+        for (int q = 0; q < (K1 + G - 1) / G; q++) {
           const int k = l + q * G;
           if (k >= K1) break;
           const float2 zk = buf[k];
@@ -570,11 +571,8 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
 
   // ---- phase D: z stencils of the products and x derivatives ----
   auto H = [&](int p, int s, int k) -> float2 { return hat[(size_t)hat_row(p, s, S) * K1 + k]; };
-  const float inv_k1 = 1.f / K1;
   for (int i = threadIdx.x; i < S * K1; i += blockDim.x) {
-    // i / K1 through the reciprocal: (i + 1/2) / K1 stays at least 1 / (2 K1)
-    // from an integer, far beyond the rounding of one product at i < 2^16
-    const int si = (int)(((float)i + 0.5f) * inv_k1), k = i - si * K1;
+    const int si = i / K1, k = i - si * K1;
     const int t = j0 + si, s = si + 1;
     if (t >= N3) continue;
     const float kxv = a.kx[k];
