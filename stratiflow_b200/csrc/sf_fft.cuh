@@ -72,16 +72,16 @@ __device__ __forceinline__ void dft(float2* v) {
 }
 
 // x: in[l + G*e] on entry, out[(l + h*G) + E*k2] in slot h*G + k2 on exit.
-// buf: this group's fft_buf_stride<N>() elements. tw: e^{-2 pi i k/kMaxN},
-// k < kMaxN. Every lane of the warp must call it together (it syncs the warp).
-template <int N, bool INV>
-__device__ __forceinline__ void reg_fft(float2 (&x)[FFTShape<N>::E], float2* buf, const float2* __restrict__ tw,
-                                        int l) {
+// buf: this group's fft_buf_stride<N>() elements. twid(k1) gives W_N^{l*k1}
+// (forward sign). Every lane of the warp must call it together (it syncs the
+// warp).
+template <int N, bool INV, class TW>
+__device__ __forceinline__ void reg_fft_body(float2 (&x)[FFTShape<N>::E], float2* buf, const TW& twid, int l) {
   constexpr int G = FFTShape<N>::G, E = FFTShape<N>::E, H = E / G;
   dft<E, INV>(x);
 #pragma unroll
   for (int k1 = 1; k1 < E; k1++) {
-    float2 w = tw[(l * k1) * (kMaxN / N)];
+    float2 w = twid(k1);
     if (INV) w.y = -w.y;
     x[k1] = cmul(x[k1], w);
   }
@@ -101,6 +101,28 @@ __device__ __forceinline__ void reg_fft(float2 (&x)[FFTShape<N>::E], float2* buf
 #pragma unroll
     for (int k2 = 0; k2 < G; k2++) x[h * G + k2] = y[h][k2];
   }
+}
+
+// the transform with the twiddles read from tw: e^{-2 pi i k/kMaxN}, k < kMaxN
+template <int N, bool INV>
+__device__ __forceinline__ void reg_fft(float2 (&x)[FFTShape<N>::E], float2* buf, const float2* __restrict__ tw,
+                                        int l) {
+  reg_fft_body<N, INV>(x, buf, [&](int k1) { return tw[(l * k1) * (kMaxN / N)]; }, l);
+}
+
+// lane l's twiddles W_N^{l*k1}, k1 < E, for a kernel that runs many
+// transforms and keeps them in registers
+template <int N>
+__device__ __forceinline__ void lane_twiddles(float2 (&w)[FFTShape<N>::E], const float2* __restrict__ tw, int l) {
+#pragma unroll
+  for (int k1 = 0; k1 < FFTShape<N>::E; k1++) w[k1] = tw[(l * k1) * (kMaxN / N)];
+}
+
+// the transform with lane_twiddles' registers
+template <int N, bool INV>
+__device__ __forceinline__ void reg_fft_w(float2 (&x)[FFTShape<N>::E], float2* buf, const float2 (&w)[FFTShape<N>::E],
+                                          int l) {
+  reg_fft_body<N, INV>(x, buf, [&](int k1) { return w[k1]; }, l);
 }
 
 // output index of register slot `slot` of lane l

@@ -353,6 +353,19 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   const int NS = S + 2;
   const int nf = tlm ? 8 : 4;   // own u1,u2,u3,b (and the base run's)
   float2* carry = reinterpret_cast<float2*>(xsm + L.carry_off);   // [4][K1]: Q1, QB, Q2, P4
+  // this lane's twiddles, held in registers for every transform of the block
+  // (read from the table at each transform when E = 32 would not fit)
+  constexpr bool kTwReg = E <= 16;
+  float2 twl[kTwReg ? E : 1];
+  if constexpr (kTwReg) lane_twiddles<N1>(twl, a.tw, l);
+  auto fft_inv = [&](float2 (&v)[E]) {
+    if constexpr (kTwReg) reg_fft_w<N1, true>(v, buf, twl, l);
+    else reg_fft<N1, true>(v, buf, a.tw, l);
+  };
+  auto fft_fwd = [&](float2 (&v)[E]) {
+    if constexpr (kTwReg) reg_fft_w<N1, false>(v, buf, twl, l);
+    else reg_fft<N1, false>(v, buf, a.tw, l);
+  };
 
   // stage the input rows u1, u2, u3, b (and the base run's) at slots s0..S+1
   // (levels jj0-1+s0 .. jj0+S) with asynchronous copies, one warp per row
@@ -423,7 +436,7 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
       }
       x[e] = zz;
     }
-    reg_fft<N1, true>(x, buf, a.tw, l);
+    fft_inv(x);
     if (valid) {
       float* rows = ofs ? bnod : nod;
       float* rA = rows + ((size_t)fA * NS + s) * N1;
@@ -498,7 +511,7 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
 #pragma unroll
           for (int e = 0; e < E; e++) x[e] = make_float2(0.f, 0.f);
       }
-      reg_fft<N1, false>(x, buf, a.tw, l);
+      fft_fwd(x);
 #pragma unroll
       for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
       __syncwarp();
@@ -551,7 +564,7 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
         x[e] = make_float2(term_eval(nod, T[0][0], n) + term_eval(nod, T[0][1], n),
                            term_eval(nod, T[1][0], n) + term_eval(nod, T[1][1], n));
       }
-      reg_fft<N1, false>(x, buf, a.tw, l);
+      fft_fwd(x);
       // natural order in the group's buffer, then split the two real transforms
 #pragma unroll
       for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
