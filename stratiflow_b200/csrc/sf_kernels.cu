@@ -14,6 +14,8 @@
 // ModalField arithmetic touches (Field.h:1129-1166).
 
 #include <algorithm>
+#include <climits>
+#include <type_traits>
 #include "sf_internal.cuh"
 #include "sf_fft.cuh"
 
@@ -702,8 +704,9 @@ __device__ __forceinline__ void load_iden(float (&bi)[K], const float* __restric
 
 // the body of k_z_cn_chunked for field f of family FAM (0: u1 and u2,
 // 1: u3, Dirichlet; 2: b), so that each family's loads and terms are fixed
-// at compile time
-template <int ZW, int FAM>
+// at compile time; IC: chunks clear of the ends take sweeps without the
+// per-level end tests
+template <int ZW, int FAM, bool IC>
 __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
   const Geo g = a.g;
   extern __shared__ float zsm[];
@@ -760,12 +763,18 @@ __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
   float bm1 = (FAM == 1 && js >= 1 && js < N3) ? bc[(js - 1) * S2] : 0.f;
   float w0 = (FAM == 2 && js < N3) ? wc[js * S2] : 0.f;
   float A = 1.f, B = 0.f;
+  // a chunk clear of both ends (levels 3..N3-4) and a whole number of batches
+  // of each sweep takes the sweeps without the per-level end tests
+  const bool interior = IC && js >= 3 && je <= N3 - 4 && (je - js) % kZI == 0;
+  static_assert(kZI % kZU2 == 0, "the first sweep's batches tile the later sweeps'");
+  auto sweep1 = [&](auto tag) {
+  constexpr bool IN = decltype(tag)::value;
   for (int j0 = js; j0 < je; j0 += kZU2) {
     float bu[kZU2], br[kZU2], bo[kZU2], bp[kZU2], bx[kZU2], bi[kZU2];
 #pragma unroll
     for (int i = 0; i < kZU2; i++) {
       const int j = j0 + i;
-      const bool in = j < je, nx = j + 1 < N3 && in;
+      const bool in = IN || j < je, nx = IN || (j + 1 < N3 && in);
       bu[i] = nx ? uc[(j + 1) * S2] : 0.f;
       br[i] = in ? rc[j * S2] : 0.f;
       bo[i] = (in && use_rold) ? rold[j * S2] : 0.f;
@@ -782,20 +791,20 @@ __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
 #pragma unroll
     for (int i = 0; i < kZU2; i++) {
       const int j = j0 + i;
-      if (j >= je) break;
+      if (!IN && j >= je) break;
       const float up = bu[i];
       float rt = br[i];
       float gp = 0.f;
       if (FAM == 0) {
         gp = sc * kgrad * bp[i];   // (i k p)_c
       } else if (FAM == 1) {
-        if (j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
+        if (IN || j >= 2) gp = dnd_lo[j] * pm1 + dnd_di[j] * bp[i];
         pm1 = bp[i];
-        if (j >= 1 && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
+        if ((IN || j >= 1) && !zmode && !a.adjoint) rt += Ri * (full_lo[j] * bm1 + full_di[j] * bx[i]);   // r3 += Ri Full(b - <b>)
         bm1 = bx[i];
       } else {
         const float w1 = bx[i];
-        const float dw = (j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
+        const float dw = (IN || j + 1 < N3) ? 0.5f * w0 + 0.5f * w1 : 0.5f * w0;
         if (!a.adjoint) rt -= dB[j] * dw;   // rB -= dB/dz ReinterpolateDirichlet(u3)
         w0 = w1;
       }
@@ -803,13 +812,13 @@ __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
       if (use_rold) R += a.hz * bo[i];
       R += -a.h * gp;
       R += a.hb * rt;
-      const bool band = dir ? (j >= 2 && j <= N3 - 2) : (j >= 1 && j <= N3 - 2);
+      const bool band = IN || (dir ? (j >= 2 && j <= N3 - 2) : (j >= 1 && j <= N3 - 2));
       const float d2u = band ? lo2[j] * um + di2[j] * u0 + up2[j] * up : 0.f;
       R += cco * ((d1 * u0 + d2 * u0) + d2u);
-      const bool zend = (j <= 1) || (j >= N3 - 2) || (dir && j == 2);   // ZeroEnds (Field.h:475-486)
+      const bool zend = !IN && ((j <= 1) || (j >= N3 - 2) || (dir && j == 2));   // ZeroEnds (Field.h:475-486)
       if (zend) R = 0.f;
       const float be = R * bi[i];
-      const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
+      const float al = (!IN && j == 0) ? 0.f : -fa[j] * bi[i];
       sD[j * 32 + lane] = be;
       if (act) rold[j * S2] = rt;
       A = al * A;
@@ -818,56 +827,69 @@ __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
       u0 = up;
     }
   }
+  };
+  if (interior) sweep1(std::true_type{});
+  else sweep1(std::false_type{});
   zscan_up<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- forward, pass 2: D_j, and with it the chunk map of the backward
   // sweep x_j = D_j - C_j x_{j+1}, composed upwards: x_js = B + A x_je ----
   float D = sIn[w * 32 + lane];
   A = 1.f;
   B = 0.f;
-  for (int j0 = js; j0 < je; j0 += kZI) {
-    float bi[kZI];
-    load_iden(bi, iden, Pp, j0, 1, js, je);
+  auto sweep2 = [&](auto tag) {
+    constexpr bool IN = decltype(tag)::value;
+    for (int j0 = js; j0 < je; j0 += kZI) {
+      float bi[kZI];
+      load_iden(bi, iden, Pp, j0, 1, IN ? INT_MIN : js, IN ? INT_MAX : je);
 #pragma unroll
-    for (int i = 0; i < kZI; i++) {
-      const int j = j0 + i;
-      if (j >= je) break;
-      const float al = (j == 0) ? 0.f : -fa[j] * bi[i];
-      D = al * D + sD[j * 32 + lane];
-      sD[j * 32 + lane] = D;
-      B = B + A * D;
-      A = -A * (fc[j] * bi[i]);
+      for (int i = 0; i < kZI; i++) {
+        const int j = j0 + i;
+        if (!IN && j >= je) break;
+        const float al = (!IN && j == 0) ? 0.f : -fa[j] * bi[i];
+        D = al * D + sD[j * 32 + lane];
+        sD[j * 32 + lane] = D;
+        B = B + A * D;
+        A = -A * (fc[j] * bi[i]);
+      }
     }
-  }
+  };
+  if (interior) sweep2(std::true_type{});
+  else sweep2(std::false_type{});
   __syncthreads();
   zscan_down<ZW>(sA, sB, sIn, w, lane, A, B);
   // ---- backward, pass 2: the solution ----
   float x = sIn[w * 32 + lane];
-  for (int j0 = je - 1; j0 >= js; j0 -= kZI) {
-    float bi[kZI];
-    load_iden(bi, iden, Pp, j0, -1, js, je);
+  auto sweep3 = [&](auto tag) {
+    constexpr bool IN = decltype(tag)::value;
+    for (int j0 = je - 1; j0 >= js; j0 -= kZI) {
+      float bi[kZI];
+      load_iden(bi, iden, Pp, j0, -1, IN ? INT_MIN : js, IN ? INT_MAX : je);
 #pragma unroll
-    for (int i = 0; i < kZI; i++) {
-      const int j = j0 - i;
-      if (j < js) break;
-      const float Cj = fc[j] * bi[i];
-      x = sD[j * 32 + lane] - Cj * x;
-      if (act) out[j * S2] = x;
+      for (int i = 0; i < kZI; i++) {
+        const int j = j0 - i;
+        if (!IN && j < js) break;
+        const float Cj = fc[j] * bi[i];
+        x = sD[j * 32 + lane] - Cj * x;
+        if (act) out[j * S2] = x;
+      }
     }
-  }
+  };
+  if (interior) sweep3(std::true_type{});
+  else sweep3(std::false_type{});
 }
 
 // k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
 // FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
-template <int ZW>
+template <int ZW, bool IC>
 __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(StageArgs a) {
   const int fi = blockIdx.y;
   const int f = a.g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
   if (f <= 1)
-    z_cn_body<ZW, 0>(a, f);
+    z_cn_body<ZW, 0, IC>(a, f);
   else if (f == 2)
-    z_cn_body<ZW, 1>(a, f);
+    z_cn_body<ZW, 1, IC>(a, f);
   else
-    z_cn_body<ZW, 2>(a, f);
+    z_cn_body<ZW, 2, IC>(a, f);
 }
 
 // RemoveDivergence with the chunked solve, for 16 modes per block: the
@@ -1244,7 +1266,8 @@ int prepare_kernels() {
   ATTR((k_xpass<128, false>)) ATTR((k_xpass<256, false>)) ATTR((k_xpass<512, false>))
   ATTR((k_xpass<16, true>)) ATTR((k_xpass<32, true>)) ATTR((k_xpass<64, true>))
   ATTR((k_xpass<128, true>)) ATTR((k_xpass<256, true>)) ATTR((k_xpass<512, true>))
-  ATTR(k_z_cn_chunked<8>) ATTR(k_z_proj_chunked<8>) ATTR(k_z_cn_chunked<16>) ATTR(k_z_proj_chunked<16>)
+  ATTR((k_z_cn_chunked<8, false>)) ATTR((k_z_cn_chunked<8, true>)) ATTR((k_z_cn_chunked<16, false>))
+  ATTR((k_z_cn_chunked<16, true>)) ATTR(k_z_proj_chunked<8>) ATTR(k_z_proj_chunked<16>)
 #undef ATTR
   return e == cudaSuccess ? 0 : -1;
 }
@@ -1255,6 +1278,24 @@ static size_t zchunk_smem(const Geo& g, int zw) { return sizeof(float) * ((size_
 // when the grid leaves SMs without a block, else 8 (three blocks per SM)
 static int z_chunks(const Geo& g, int fields) {
   return (long long)cdiv(g.P, 16) * fields * g.nrun < 148 ? 16 : 8;
+}
+
+// the CN solves of a stage; chunks of 48 levels or more take the variant
+// with end-test-free interior sweeps (measured 7% faster at 384 levels in 8
+// chunks, and slower with 32-level chunks, where it is not used)
+static void launch_z_cn(const StageArgs& a, cudaStream_t st) {
+  const Geo& g = a.g;
+  const int nf = g.dim3 ? 4 : 3;
+  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
+  const int zw = z_chunks(g, nf);
+  const bool ic = cdiv(g.N3, zw) >= 48;
+  if (zw == 16) {
+    if (ic) k_z_cn_chunked<16, true><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+    else k_z_cn_chunked<16, false><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+  } else {
+    if (ic) k_z_cn_chunked<8, true><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+    else k_z_cn_chunked<8, false><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+  }
 }
 
 int launch_project(const StageArgs& a, cudaStream_t st) {
@@ -1293,12 +1334,7 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     launch_fft_y(a, st);
     mark();
   }
-  const int nf = g.dim3 ? 4 : 3;
-  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
-  if (z_chunks(g, nf) == 16)
-    k_z_cn_chunked<16><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
-  else
-    k_z_cn_chunked<8><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+  launch_z_cn(a, st);
   mark();
   launch_project(a, st);
   mark();
@@ -1306,13 +1342,7 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
 }
 
 int launch_z_solves(const StageArgs& a, cudaStream_t st) {
-  const Geo& g = a.g;
-  const int nf = g.dim3 ? 4 : 3;
-  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
-  if (z_chunks(g, nf) == 16)
-    k_z_cn_chunked<16><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
-  else
-    k_z_cn_chunked<8><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+  launch_z_cn(a, st);
   launch_project(a, st);
   return 2;
 }
