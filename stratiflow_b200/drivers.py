@@ -37,6 +37,12 @@ def load_host():
         L.sfh_arnoldi.restype = C.c_int
         L.sfh_full_evolve.argtypes = [C.c_void_p, d, d, i, dp]
         L.sfh_full_evolve.restype = C.c_int
+        L.sfh_linear_evolve.argtypes = [dp, fp, fp, d, fp]
+        L.sfh_inverse_iteration.argtypes = [dp, fp, fp, d, d, d, i, i, dp, i]
+        L.sfh_critical_point.argtypes = [dp, i, d, d, fp, dp, dp, dp, i]
+        L.sfh_find_hopf.argtypes = [dp, i, d, fp, dp, dp, dp, dp, i]
+        for f in ("sfh_linear_evolve", "sfh_inverse_iteration", "sfh_critical_point", "sfh_find_hopf"):
+            getattr(L, f).restype = C.c_int
         for f in ("sfh_newton_fixed", "sfh_periodic_orbit", "sfh_arclength", "sfh_evolve", "sfh_evolve_tangent"):
             getattr(L, f).restype = C.c_int
         _host = L
@@ -206,6 +212,119 @@ def arnoldi(flow: Flow, about, T=11.0, block=16, krylov=320, tol=1e-6, nev=6, se
     ev = re[:n.value] + 1j * im[:n.value]
     stats = {"directions": int(st[0]), "integrations": int(st[1]), "seconds": float(st[2])}
     return (ev, vr, vi, stats) if vectors else (ev, stats)
+
+
+# ---------------------------------------------------------- bifurcations
+def linear_evolve(flow: Flow, about, d, T, Ri=None):
+    """LinearEvolve (StateVector.cpp:107-156): d advanced over T by
+    TimeStepLinear about the frozen state `about` (SetBackground,
+    IMEXRK.h:334-352), in equal steps of at most flow.dt."""
+    L = load_host()
+    f = _flow_at(flow, Ri)
+    a = np.ascontiguousarray(np.asarray(about, dtype=np.complex64).reshape(flow.state_shape))
+    x = np.ascontiguousarray(np.asarray(d, dtype=np.complex64).reshape(flow.state_shape))
+    out = np.zeros_like(x)
+    _call(L.sfh_linear_evolve(_dp(f.array()), _fp(a), _fp(x), float(T), _fp(out)))
+    return out
+
+
+def _flow_at(flow: Flow, Ri):
+    if Ri is None:
+        return flow
+    f = Flow(flow.N1, flow.N2, flow.N3, flow.L1, flow.L2, flow.L3, flow.Re, flow.Pr, Ri, flow.dt, flow.background)
+    return f
+
+
+def inverse_iteration(flow: Flow, about, b0, T=5.0, mu=1.0, eps=0.05, iters=5, krylov=512, Ri=None):
+    """InverseIteration (InverseIteration.cpp:1-124): the eigenvector of the
+    linearised evolution over T about `about` whose eigenvalue is nearest mu,
+    from the start b0. Each iteration solves (L - mu) y = b by GMRES to
+    relative residual eps and normalises. Returns (b, history) with history
+    {"eigenvalue": |L b| / |b| before each solve, "residual": |L b -
+    eigenvalue b|, "krylov": GMRES vectors of each solve}."""
+    L = load_host()
+    f = _flow_at(flow, Ri)
+    a = np.ascontiguousarray(np.asarray(about, dtype=np.complex64).reshape(flow.state_shape))
+    b = np.ascontiguousarray(np.asarray(b0, dtype=np.complex64).reshape(flow.state_shape)).copy()
+    hist = np.zeros(1 + 3 * iters)
+    _call(L.sfh_inverse_iteration(_dp(f.array()), _fp(a), _fp(b), float(T), float(mu), float(eps), int(iters),
+                                  int(krylov), _dp(hist), len(hist)))
+    n = int(hist[0])
+    return b, {"eigenvalue": list(hist[1:1 + n]), "residual": list(hist[1 + n:1 + 2 * n]),
+               "krylov": [int(v) for v in hist[1 + 2 * n:1 + 3 * n]]}
+
+
+def _critical(flow, mode, x, v, Ri, T, weight, opts):
+    L = load_host()
+    xv = np.ascontiguousarray(np.stack([np.asarray(x, dtype=np.complex64).reshape(flow.state_shape),
+                                        np.asarray(v, dtype=np.complex64).reshape(flow.state_shape)]))
+    ri = np.array([Ri], dtype=np.float64)
+    st = np.zeros(8 + 3 * 64)
+    ov = (opts or NKOptions(jacobian="fd", block=0)).v.copy()
+    ov[7] = 0
+    _call(L.sfh_critical_point(_dp(flow.array()), int(mode), float(T), float(weight), _fp(xv), _dp(ri), _dp(ov),
+                               _dp(st), len(st)))
+    return xv[0], xv[1], float(ri[0]), st
+
+
+def find_critical_point(flow: Flow, x, v, Ri, T=11.0, weight=1.0, opts: NKOptions | None = None):
+    """FindCriticalPoint (FindCriticalPoint.cpp:110-213): a state x, an
+    eigenvector v with eigenvalue 1 of the evolution over T linearised about
+    x, and the Ri at which they exist, by Newton-Krylov (finite-difference
+    Jacobian actions, as the reference's NewtonKrylov) on F = (Phi_T(x) - x,
+    L_T(x) v - v, Energy(v) - weight) after the constraints (v orthogonal to
+    ddx x, mean of u1 and b removed, Energy(v) = weight).
+    Returns (x, v, Ri, stats)."""
+    x, v, ri, st = _critical(flow, 0, x, v, Ri, T, weight, opts)
+    return x, v, ri, _stats(st)
+
+
+def critical_point_constraints(flow: Flow, x, v, Ri, weight=1.0):
+    """FindCriticalPoint::EnforceConstraints (FindCriticalPoint.cpp:114-134) alone."""
+    x, v, ri, _ = _critical(flow, 1, x, v, Ri, 1.0, weight, None)
+    return x, v, ri
+
+
+def critical_point_function(flow: Flow, x, v, Ri, T=11.0, weight=1.0):
+    """FindCriticalPoint::EvalFunction (FindCriticalPoint.cpp:136-150): (F_x, F_v, F_p)."""
+    return _critical(flow, 2, x, v, Ri, T, weight, None)[:3]
+
+
+def _hopf(flow, mode, x, v1, v2, Ri, theta, T, opts):
+    L = load_host()
+    xv = np.ascontiguousarray(np.stack([np.asarray(a, dtype=np.complex64).reshape(flow.state_shape)
+                                        for a in (x, v1, v2)]))
+    ri = np.array([Ri], dtype=np.float64)
+    th = np.array([theta], dtype=np.float64)
+    st = np.zeros(8 + 3 * 64)
+    ov = (opts or NKOptions(jacobian="fd", block=0)).v.copy()
+    ov[7] = 0
+    _call(L.sfh_find_hopf(_dp(flow.array()), int(mode), float(T), _fp(xv), _dp(ri), _dp(th), _dp(ov), _dp(st),
+                          len(st)))
+    return xv[0], xv[1], xv[2], float(ri[0]), float(th[0]), st
+
+
+def find_hopf(flow: Flow, x, v1, v2, Ri, theta, T=11.0, opts: NKOptions | None = None):
+    """FindHopf (FindHopf.cpp:4-101): a state x and a complex eigenvector
+    v1 + i v2 with eigenvalue exp(i theta) (modulus 1) of the evolution over
+    T linearised about x, and the Ri at which they exist, by Newton-Krylov
+    with finite-difference Jacobian actions. v1, v2 are first divided by |v1|
+    and A = v1 fixes the eigenvector's phase and size (v1.A = 1, v2.A = 0).
+    Returns (x, v1, v2, Ri, theta, stats)."""
+    x, v1, v2, ri, th, st = _hopf(flow, 0, x, v1, v2, Ri, theta, T, opts)
+    return x, v1, v2, ri, th, _stats(st)
+
+
+def hopf_constraints(flow: Flow, x, v1, v2, Ri, theta):
+    """FindHopf::EnforceConstraints (FindHopf.cpp:9-20) after the initial
+    rescaling by |v1| (FindHopf.cpp:88-93)."""
+    return _hopf(flow, 1, x, v1, v2, Ri, theta, 1.0, None)[:5]
+
+
+def hopf_function(flow: Flow, x, v1, v2, Ri, theta, T=11.0):
+    """FindHopf::EvalFunction (FindHopf.cpp:22-50) after the initial
+    rescaling by |v1|: (F_x, F_v1, F_v2, F_p = v2.A, F_theta = v1.A - 1)."""
+    return _hopf(flow, 2, x, v1, v2, Ri, theta, T, None)[:5]
 
 
 # ------------------------------------------------------------ continuation

@@ -4,6 +4,10 @@
 //   sfh_periodic_orbit   FindPeriodic (FindPeriodic.cpp): Phi_T(x) = x, T unknown
 //   sfh_arclength        one corrector of PseudoArclength (PseudoArclength.cpp:63-68)
 //   sfh_arnoldi          BasicArnoldi (Arnoldi.h:15-226): eigenvalues of the linearised evolution
+//   sfh_linear_evolve    LinearEvolve (StateVector.cpp:107-156) about a frozen state
+//   sfh_inverse_iteration  InverseIteration (InverseIteration.cpp)
+//   sfh_critical_point   FindCriticalPoint (FindCriticalPoint.cpp)
+//   sfh_find_hopf        FindHopf (FindHopf.cpp)
 // States cross this interface in the kept layout of include/stratiflow_b200.h,
 // M consecutive states (the shooting segments).
 #include <cstring>
@@ -266,6 +270,133 @@ int sfh_arnoldi(const double* params, const float* about, double T, int block, i
       stats[1] = (double)r.integrations;
       stats[2] = r.seconds;
     }
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// LinearEvolve (StateVector.cpp:107-156): d advanced over T by TimeStepLinear
+// about the frozen state `about`, into out (one state each, kept layout)
+int sfh_linear_evolve(const double* params, const float* about, const float* d, double T, float* out) {
+  try {
+    Params p = params_from(params);
+    Context c(p, 1);
+    Vec a(c), x(c);
+    load(a, about, p);
+    load(x, d, p);
+    LinearEvolveSegment(a, 0, x, 0, T, p.Ri, x, 0);
+    store(x, out, p);
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// InverseIteration (InverseIteration.cpp:1-124) about `about` at the Ri of
+// params: b (one state) in and out, normalised; shift mu, GMRES tolerance
+// eps, at most `krylov` vectors per solve. hist: [0] iterations n, then n
+// eigenvalue estimates, n residuals, n GMRES vector counts.
+int sfh_inverse_iteration(const double* params, const float* about, float* b, double T, double mu, double eps,
+                          int iters, int krylov, double* hist, int cap) {
+  try {
+    Params p = params_from(params);
+    Context c(p, 1);
+    Vec a(c), x(c);
+    load(a, about, p);
+    load(x, b, p);
+    x.EnforceBCs();
+    InverseIterationResult r = InverseIteration(a, x, T, mu, eps, iters, krylov);
+    store(x, b, p);
+    const int n = (int)r.mu.size();
+    if (hist && cap >= 1 + 3 * n) {
+      hist[0] = n;
+      for (int i = 0; i < n; i++) {
+        hist[1 + i] = r.mu[i];
+        hist[1 + n + i] = r.residual[i];
+        hist[1 + 2 * n + i] = r.krylov[i];
+      }
+    }
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// FindCriticalPoint (FindCriticalPoint.cpp:110-213): xv = (x, v), two states
+// in and out; *Ri the parameter unknown p, in and out. mode 0: the
+// constraints, then Newton-Krylov (the reference's main, :203-208); 1: the
+// constraints only; 2: F(x, v, Ri) into xv and *Ri.
+int sfh_critical_point(const double* params, int mode, double T, double weight, float* xv, double* Ri,
+                       const double* opts, double* stats, int cap) {
+  try {
+    Params p = params_from(params);
+    p.Ri = *Ri;
+    Context c(p, 2);
+    Vec x(c);
+    load(x, xv, p);
+    x.EnforceBCs();
+    x.p = *Ri;
+    CriticalPointNK nk(options_from(opts), T, weight);
+    if (mode == 2) {
+      Vec F = nk.EvalFunction(x);
+      store(F, xv, p);
+      *Ri = F.p;
+      return 0;
+    }
+    nk.EnforceConstraints(x);
+    if (mode == 0) {
+      NKStats st = nk.Run(x);
+      write_stats(st, stats, cap);
+    }
+    store(x, xv, p);
+    *Ri = x.p;
+    return 0;
+  } catch (const std::exception& e) {
+    g_host_err = e.what();
+    return -1;
+  }
+}
+
+// FindHopf (FindHopf.cpp:4-101): xv = (x, v1, v2), three states in and out;
+// *Ri (p) and *theta (the eigenvalue's argument) in and out. v1 and v2 are
+// first divided by |v1| and A is the resulting v1 (:88-93). mode 0: the
+// constraints, then Newton-Krylov; 1: the constraints only; 2: F into xv,
+// *theta (v1.A - 1) and *Ri (v2.A).
+int sfh_find_hopf(const double* params, int mode, double T, float* xv, double* Ri, double* theta,
+                  const double* opts, double* stats, int cap) {
+  try {
+    Params p = params_from(params);
+    p.Ri = *Ri;
+    Context c(p, 3);
+    Vec x(c);
+    load(x, xv, p);
+    x.EnforceBCs();
+    x.p = *Ri;
+    x.q = *theta;
+    const double n1 = std::sqrt(SegmentDot(x, x, 1));
+    if (n1 > 0) check(sf_vecs_scale(x.v(), 1, 1.0 / n1, 2));
+    Vec A(c);
+    check(sf_vecs_copy(A.v(), 0, x.v(), 1));
+    HopfNK nk(options_from(opts), T, A);
+    if (mode == 2) {
+      Vec F = nk.EvalFunction(x);
+      store(F, xv, p);
+      *Ri = F.p;
+      *theta = F.q;
+      return 0;
+    }
+    nk.EnforceConstraints(x);
+    if (mode == 0) {
+      NKStats st = nk.Run(x);
+      write_stats(st, stats, cap);
+    }
+    store(x, xv, p);
+    *Ri = x.p;
+    *theta = x.q;
     return 0;
   } catch (const std::exception& e) {
     g_host_err = e.what();

@@ -154,6 +154,17 @@ struct Context {
     }
     return *tangent;
   }
+  // one-run solvers for segment-wise evolutions: the nonlinear map, and
+  // TimeStepLinear about a frozen base (LinearEvolve, StateVector.cpp:107-156)
+  std::unique_ptr<Solver> single, linear;
+  Solver& single_solver() {
+    if (!single) single.reset(new Solver(p, 1));
+    return *single;
+  }
+  Solver& linear_solver() {
+    if (!linear) linear.reset(new Solver(p, 1));
+    return *linear;
+  }
   // one base and s tangent-linear runs (block Krylov methods, M = 1)
   std::unique_ptr<Solver> block_tangent;
   Solver& block_tangent_solver(int s) {
@@ -170,17 +181,19 @@ struct Context {
 class Vec {
  public:
   explicit Vec(Context& c) : c_(&c), s_(new Store(*c.solver, c.M)) {}
-  Vec(const Vec& o) : c_(o.c_), s_(new Store(*o.c_->solver, o.c_->M)), p(o.p) {
+  Vec(const Vec& o) : c_(o.c_), s_(new Store(*o.c_->solver, o.c_->M)), p(o.p), q(o.q) {
     check(sf_vecs_copy_range(o));
   }
   Vec& operator=(const Vec& o) {
     if (this != &o) {
       check(sf_vecs_copy_range(o));
       p = o.p;
+      q = o.q;
     }
     return *this;
   }
   double p = 0.0;
+  double q = 0.0;   // a second scalar unknown (the Hopf frequency theta, HopfBifurcation.h:12-14); 0 elsewhere
 
   int M() const { return c_->M; }
   sf_vecs* v() const { return s_->v(); }
@@ -190,6 +203,7 @@ class Vec {
   void MulAdd(double a, const Vec& x) {
     check(sf_vecs_axpy(v(), 0, a, x.v(), 0, M()));
     p += a * x.p;
+    q += a * x.q;
     EnforceBCs();
   }
   Vec& operator+=(const Vec& x) { MulAdd(1.0, x); return *this; }
@@ -197,19 +211,21 @@ class Vec {
   Vec& operator*=(double a) {
     check(sf_vecs_scale(v(), 0, a, M()));
     p *= a;
+    q *= a;
     return *this;
   }
   // StateVector::Dot summed over the segments + p p' (ExtendedStateVector.h:12-15)
   double Dot(const Vec& o, bool with_p = true) const {
     double d = 0;
     check(sf_vecs_dot_sum(v(), 0, o.v(), 0, M(), c_->p.Ri, &d));
-    return d + (with_p ? p * o.p : 0.0);
+    return d + (with_p ? p * o.p + q * o.q : 0.0);
   }
   double Norm2() const { return Dot(*this); }
   double Norm() const { return std::sqrt(Norm2()); }
   void Zero() {
     check(sf_vecs_scale(v(), 0, 0.0, M()));
     p = 0;
+    q = 0;
   }
   void EnforceBCs() { check(sf_vecs_enforce_bcs(v(), 0, M())); }
   // RemovePhaseShift of segment 0, the same shift applied to every segment
@@ -1761,5 +1777,281 @@ class BlockArnoldi {
     check(sf_vecs_enforce_bcs(W.v(), 0, W.n()));
   }
 };
+
+// ====================================================== bifurcations ====
+// The drivers of InverseIteration.cpp, FindCriticalPoint.cpp and FindHopf.cpp.
+// Their extended states are one Vec whose segments are the state and its
+// eigenvector(s): the reference's CriticalPoint (x, v, p) and
+// HopfBifurcation (x, v1, v2, theta, p) have exactly the inner product, the
+// MulAdd and the EnforceBCs of a Vec of two or three segments with p (and
+// q = theta). The state segment evolves by FullEvolve and the eigenvector
+// segments by LinearEvolve about the frozen state, one segment at a time.
+
+inline int steps_over(const Context& c, double tau) { return std::max(1, (int)std::ceil(tau / c.p.dt - 1e-9)); }
+
+// FullEvolve (StateVector.cpp:3-84) of segment i of x into segment o of out,
+// as Evolve does for all segments: p zeroed, projected, equal steps of at
+// most dt, EnforceBCs on the result
+inline void EvolveSegment(const Vec& x, int i, double tau, double Ri, Vec& out, int o) {
+  Context& c = x.ctx();
+  auto t0 = std::chrono::steady_clock::now();
+  Solver& s = c.single_solver();
+  const int n = steps_over(c, tau);
+  s.set_dt(tau / n);
+  s.set_ri(0, Ri);
+  if (&out != &x || o != i) check(sf_vecs_copy(out.v(), o, x.v(), i));
+  check(sf_vecs_zero_pressure(out.v(), o, 1));
+  check(sf_vecs_to_run(out.v(), o, s.h(), 0, 1));
+  check(sf_prepare(s.h()));
+  check(sf_step(s.h(), n));
+  check(sf_vecs_from_run(out.v(), o, s.h(), 0, 1));
+  check(sf_vecs_enforce_bcs(out.v(), o, 1));
+  check(sf_vecs_synchronize(out.v()));
+  c.evolutions += 1;
+  c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// LinearEvolve (StateVector.cpp:107-156): segment id of d advanced over tau
+// by TimeStepLinear about the frozen base segment ia of `about`
+// (SetBackground, IMEXRK.h:334-352), into segment o of out. The steps are
+// those of EvolveSegment (the reference fixes deltaT = 0.01 here).
+inline void LinearEvolveSegment(const Vec& about, int ia, const Vec& d, int id, double tau, double Ri, Vec& out,
+                                int o) {
+  Context& c = about.ctx();
+  auto t0 = std::chrono::steady_clock::now();
+  Solver& s = c.linear_solver();
+  const int n = steps_over(c, tau);
+  s.set_dt(tau / n);
+  s.set_ri(0, Ri);
+  void* base = nullptr;
+  check(sf_vecs_device(about.v(), ia, &base));
+  check(sf_set_base_device(s.h(), 0, base));
+  if (&out != &d || o != id) check(sf_vecs_copy(out.v(), o, d.v(), id));
+  check(sf_vecs_zero_pressure(out.v(), o, 1));
+  check(sf_vecs_to_run(out.v(), o, s.h(), 0, 1));
+  check(sf_prepare(s.h()));
+  check(sf_step_linear(s.h(), n));
+  check(sf_vecs_from_run(out.v(), o, s.h(), 0, 1));
+  check(sf_vecs_enforce_bcs(out.v(), o, 1));
+  check(sf_vecs_synchronize(out.v()));
+  c.evolutions += 1;
+  c.evolve_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// CopyToSolver, FilterAll, PopulateNodalVariables, RemoveDivergence(0),
+// CopyFromSolver of segment i (the projection Rescale brackets its scaling
+// with, StateVector.cpp:189-226); p is zeroed
+inline void ProjectSegment(Vec& x, int i) {
+  Solver& s = x.ctx().single_solver();
+  check(sf_vecs_zero_pressure(x.v(), i, 1));
+  check(sf_vecs_to_run(x.v(), i, s.h(), 0, 1));
+  check(sf_prepare(s.h()));
+  check(sf_vecs_from_run(x.v(), i, s.h(), 0, 1));
+}
+
+// StateVector::Rescale (StateVector.cpp:189-226) of segment i to `energy`
+// (Energy = Dot / 2, StateVector.h:141-144)
+inline void RescaleSegment(Vec& x, int i, double energy) {
+  ProjectSegment(x, i);
+  const double e = 0.5 * SegmentDot(x, x, i);
+  check(sf_vecs_scale(x.v(), i, e != 0.0 ? std::sqrt(energy / e) : 0.0, 1));
+  ProjectSegment(x, i);
+}
+
+// ddx of u1, u2, u3, b of segment i into segment o of out (i kx on every
+// kept mode m = q K1 + j1, kx = 2 pi j1 / L1); p zero
+inline void DdxSegment(const Vec& x, int i, Vec& out, int o) {
+  const Params& P = x.ctx().p;
+  const int K1 = P.N1 / 3, K2 = P.N2 > 1 ? 2 * (P.N2 / 3) - 1 : 1;
+  const int plane = (K1 * K2 + 15) / 16 * 16;
+  const size_t n = (size_t)5 * P.N3 * plane;
+  std::vector<float> h(2 * n);
+  x.get_segment_host(i, h.data());
+  const double two_pi = 2.0 * std::acos(-1.0);
+  for (int f = 0; f < 5; f++)
+    for (int t = 0; t < P.N3; t++)
+      for (int m = 0; m < plane; m++) {
+        float* z = h.data() + 2 * (((size_t)f * P.N3 + t) * plane + m);
+        if (f == 4 || m >= K1 * K2) {
+          z[0] = z[1] = 0.f;
+          continue;
+        }
+        const float kx = (float)(two_pi * (m % K1) / P.L1);
+        const float re = z[0], im = z[1];
+        z[0] = -kx * im;
+        z[1] = kx * re;
+      }
+  out.set_segment_host(o, h.data());
+}
+
+// FindCriticalPoint (FindCriticalPoint.cpp:110-150): unknowns x (segment 0),
+// v (segment 1) and p = Ri; F = (Phi_T(x) - x, L_T(x) v - v, Energy(v) -
+// weight), L_T(x) the evolution linearised about the frozen x. The
+// constraints take the component along ddx x (the shift symmetry) and the
+// mean of u1 and b out of v and rescale it to the weight. Every evaluation
+// sets the Ri of the inner products to p, as the reference sets flowParams.Ri.
+class CriticalPointNK : public NewtonKrylov {
+ public:
+  CriticalPointNK(const NKOptions& o, double T, double weight) : NewtonKrylov(o), T_(T), weight_(weight) {}
+  Vec EvalFunction(const Vec& at) override {
+    Context& c = at.ctx();
+    c.p.Ri = at.p;
+    Vec r(at);
+    EvolveSegment(at, 0, T_, at.p, r, 0);
+    LinearEvolveSegment(at, 0, at, 1, T_, at.p, r, 1);
+    r.MulAdd(-1.0, at);
+    r.p = 0.5 * SegmentDot(at, at, 1) - weight_;
+    r.q = 0;
+    return r;
+  }
+  void EnforceConstraints(Vec& at) override {
+    Context& c = at.ctx();
+    c.p.Ri = at.p;
+    Vec ps(at);
+    DdxSegment(at, 0, ps, 0);
+    const double n2 = SegmentDot(ps, ps, 0);
+    if (n2 != 0) {
+      double d = 0;
+      check(sf_vecs_dots(at.v(), 1, 1, ps.v(), 0, c.p.Ri, &d));
+      check(sf_vecs_axpy(at.v(), 1, -d / n2, ps.v(), 0, 1));
+    }
+    check(sf_vecs_remove_average(at.v(), 1, 0, c.p.L3));
+    check(sf_vecs_remove_average(at.v(), 1, 3, c.p.L3));
+    RescaleSegment(at, 1, weight_);
+  }
+
+ private:
+  double T_, weight_;
+};
+
+// FindHopf (FindHopf.cpp:4-57): unknowns x, v1, v2 (segments 0, 1, 2),
+// q = theta and p = Ri; F = (Phi_T(x) - x, L v1 - cos(theta) v1 + sin(theta)
+// v2, L v2 - sin(theta) v1 - cos(theta) v2, v1.A - 1, v2.A), A the first
+// eigenvector of the initial guess (segment 0 of `A`). The constraint turns
+// (v1, v2) in their plane so that v1.A = 1 and v2.A = 0.
+class HopfNK : public NewtonKrylov {
+ public:
+  HopfNK(const NKOptions& o, double T, const Vec& A) : NewtonKrylov(o), T_(T), A_(A) {}
+  Vec EvalFunction(const Vec& at) override {
+    Context& c = at.ctx();
+    c.p.Ri = at.p;
+    Vec r(at);
+    EvolveSegment(at, 0, T_, at.p, r, 0);
+    LinearEvolveSegment(at, 0, at, 1, T_, at.p, r, 1);
+    LinearEvolveSegment(at, 0, at, 2, T_, at.p, r, 2);
+    const double cs = std::cos(at.q), sn = std::sin(at.q);
+    check(sf_vecs_axpy(r.v(), 0, -1.0, at.v(), 0, 1));
+    check(sf_vecs_axpy(r.v(), 1, -cs, at.v(), 1, 1));
+    check(sf_vecs_axpy(r.v(), 1, sn, at.v(), 2, 1));
+    check(sf_vecs_axpy(r.v(), 2, -sn, at.v(), 1, 1));
+    check(sf_vecs_axpy(r.v(), 2, -cs, at.v(), 2, 1));
+    r.EnforceBCs();
+    r.q = ADot(at, 1) - 1.0;
+    r.p = ADot(at, 2);
+    return r;
+  }
+  void EnforceConstraints(Vec& at) override {
+    at.ctx().p.Ri = at.p;
+    const double a1 = ADot(at, 1), a2 = ADot(at, 2);
+    const double th = std::atan2(-a2, a1);
+    const double r = 1.0 / (std::cos(th) * a1 - std::sin(th) * a2);
+    Vec old(at);
+    // v1 <- r cos v1 - r sin v2, v2 <- r sin v1 + r cos v2 (the old v1, v2)
+    check(sf_vecs_lincomb(at.v(), 1, r * std::cos(th), -r * std::sin(th), old.v(), 2, 1));
+    check(sf_vecs_lincomb(at.v(), 2, r * std::cos(th), r * std::sin(th), old.v(), 1, 1));
+  }
+  double ADot(const Vec& at, int seg) const {
+    double d = 0;
+    check(sf_vecs_dots(at.v(), seg, 1, A_.v(), 0, at.ctx().p.Ri, &d));
+    return d;
+  }
+
+ private:
+  double T_;
+  Vec A_;
+};
+
+struct InverseIterationResult {
+  std::vector<double> mu;         // |L b| / |b| before each solve (muApprox)
+  std::vector<double> residual;   // |L b - muApprox b| with |b| = 1
+  std::vector<int> krylov;        // GMRES vectors of each solve
+};
+
+// InverseIteration (InverseIteration.cpp:1-124) about the frozen state
+// `about` (one segment): each iteration reports muApprox = |L b| / |b| and
+// the residual |L b - muApprox b|, solves (L - mu) y = b by GMRES (modified
+// Gram-Schmidt, EnforceBCs on each basis vector) to relative residual eps
+// with at most K vectors, and takes b = y / |y|. The reference solves each
+// least-squares problem by an SVD of the Hessenberg block; Givens rotations
+// give the same minimiser (the block has full rank while the basis grows)
+// at O(k) work per vector instead of O(k^3).
+inline InverseIterationResult InverseIteration(const Vec& about, Vec& b, double T, double mu, double eps, int iters,
+                                               int K) {
+  Context& c = about.ctx();
+  const double Ri = c.p.Ri;
+  InverseIterationResult out;
+  b *= 1.0 / b.Norm();
+  for (int it = 0; it < iters; it++) {
+    Vec bT(b);
+    LinearEvolveSegment(about, 0, b, 0, T, Ri, bT, 0);
+    const double ma = bT.Norm() / b.Norm();
+    bT.MulAdd(-ma, b);
+    out.mu.push_back(ma);
+    out.residual.push_back(bT.Norm());
+    if (verbose()) std::fprintf(stderr, "Inverse iteration %d: eigenvalue %.8f, residual %.3e\n", it, ma, bT.Norm());
+    std::vector<std::unique_ptr<Vec>> q;
+    q.emplace_back(new Vec(b));
+    q[0]->EnforceBCs();
+    const double beta = q[0]->Norm();
+    *q[0] *= 1.0 / beta;
+    // Hessenberg columns, reduced by Givens rotations as they arrive
+    std::vector<std::vector<double>> R;
+    std::vector<double> cs, sn, g(1, beta);
+    int used = 0;
+    for (int k = 1; k < K; k++) {
+      q.emplace_back(new Vec(*q[k - 1]));
+      LinearEvolveSegment(about, 0, *q[k - 1], 0, T, Ri, *q[k], 0);
+      q[k]->MulAdd(-mu, *q[k - 1]);
+      std::vector<double> h(k + 1, 0.0);
+      for (int j = 0; j < k; j++) {
+        h[j] = q[j]->Dot(*q[k]);
+        q[k]->MulAdd(-h[j], *q[j]);
+      }
+      h[k] = q[k]->Norm();
+      if (h[k] > 0) *q[k] *= 1.0 / h[k];
+      q[k]->EnforceBCs();
+      used = k;
+      for (int j = 0; j < k - 1; j++) {   // earlier rotations
+        const double a = h[j], bb = h[j + 1];
+        h[j] = cs[j] * a + sn[j] * bb;
+        h[j + 1] = -sn[j] * a + cs[j] * bb;
+      }
+      const double rr = std::hypot(h[k - 1], h[k]);
+      const double cj = rr > 0 ? h[k - 1] / rr : 1.0, sj = rr > 0 ? h[k] / rr : 0.0;
+      cs.push_back(cj);
+      sn.push_back(sj);
+      h[k - 1] = rr;
+      h[k] = 0;
+      g.push_back(-sj * g[k - 1]);
+      g[k - 1] = cj * g[k - 1];
+      R.push_back(h);
+      const double res = std::fabs(g[k]) / beta;
+      if (verbose() && k % 10 == 0) std::fprintf(stderr, "GMRES STEP %d, RESIDUAL: %.3e\n", k, res);
+      if (res < eps || !(rr > 0)) break;
+    }
+    // back substitution R y = g, then b = sum y_k q_k
+    std::vector<double> y(used, 0.0);
+    for (int i = used - 1; i >= 0; i--) {
+      double s = g[i];
+      for (int j = i + 1; j < used; j++) s -= R[j][i] * y[j];
+      y[i] = R[i][i] != 0 ? s / R[i][i] : 0.0;
+    }
+    b.Zero();
+    for (int k = 0; k < used; k++) b.MulAdd(y[k], *q[k]);
+    b *= 1.0 / b.Norm();
+    out.krylov.push_back(used);
+  }
+  return out;
+}
 
 }  // namespace stratiflow
