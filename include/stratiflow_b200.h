@@ -102,6 +102,16 @@ int sf_get_field(sf_solver* s, int run, int field, float* ref_layout);
 int sf_set_state_kept(sf_solver* s, const float* host);
 int sf_get_state_kept(sf_solver* s, float* host);
 
+/* CopyToSolver, nsteps x TimeStep, CopyFromSolver (StateVector.h:511-543 around
+ * IMEXRK::TimeStep, IMEXRK.cpp:5-24) for a stream of independent states held in
+ * host memory: enqueues the copy of host_in (all runs, kept layout) to the
+ * device, the steps, and the copy of the result to host_out, and returns.
+ * Consecutive calls overlap: the input copy of call k+1 and the output copy of
+ * call k-1 run on their own streams while call k steps (two device staging
+ * buffers per direction). host_in must stay unchanged and host_out unread until
+ * sf_synchronize; pinned host memory makes the copies asynchronous. */
+int sf_step_host_async(sf_solver* s, const float* host_in, float* host_out, int nsteps);
+
 /* device pointer of the current state in the kept layout (valid until the
  * next step call), and its size in bytes */
 int sf_state_device(sf_solver* s, void** dptr, size_t* bytes);

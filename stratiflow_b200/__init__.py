@@ -26,7 +26,7 @@ FIELD = {"u1": U1, "u2": U2, "u3": U3, "b": B, "p": P}
 # every entry point declared in include/stratiflow_b200.h
 EXPORTS = [
     "sf_create", "sf_destroy", "sf_last_error", "sf_set_dt", "sf_set_ri", "sf_set_background",
-    "sf_set_field", "sf_get_field", "sf_set_state_kept", "sf_get_state_kept", "sf_state_device",
+    "sf_set_field", "sf_get_field", "sf_set_state_kept", "sf_get_state_kept", "sf_step_host_async", "sf_state_device",
     "sf_set_state_device", "sf_prepare", "sf_remove_divergence", "sf_step", "sf_set_base",
     "sf_step_linear", "sf_energy", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
     "sf_profile_step", "sf_profile_names", "sf_remove_divergence_noalloc",
@@ -73,6 +73,7 @@ def load_library(path: str | None = None):
         "sf_destroy": [vp], "sf_set_dt": [vp, d], "sf_set_ri": [vp, i, d],
         "sf_set_background": [vp, i, dp, dp], "sf_set_field": [vp, i, i, fp],
         "sf_get_field": [vp, i, i, fp], "sf_set_state_kept": [vp, fp], "sf_get_state_kept": [vp, fp],
+        "sf_step_host_async": [vp, fp, fp, i],
         "sf_state_device": [vp, C.POINTER(vp), C.POINTER(C.c_size_t)], "sf_set_state_device": [vp, vp],
         "sf_prepare": [vp], "sf_remove_divergence": [vp, d], "sf_step": [vp, i],
         "sf_set_base": [vp, i, fp, fp, fp, fp], "sf_step_linear": [vp, i],
@@ -210,6 +211,16 @@ class IMEXRK:
             out = np.zeros(self.kept_shape, dtype=np.complex64)
         _check(load_library().sf_get_state_kept(self._h, _fptr(out)))
         return out
+
+    def step_host_async(self, host_in, host_out, n=1):
+        """sf_step_host_async: copy host_in (kept layout, all runs) in, n x
+        TimeStep, copy the result to host_out, without waiting; consecutive
+        calls overlap their copies with each other's steps. The arrays must
+        stay alive, host_in unchanged and host_out unread until synchronize()."""
+        for a in (host_in, host_out):
+            if a.dtype != np.complex64 or a.size != int(np.prod(self.kept_shape)) or not a.flags.c_contiguous:
+                raise SFError("step_host_async takes contiguous complex64 arrays of the kept shape")
+        _check(load_library().sf_step_host_async(self._h, _fptr(host_in), _fptr(host_out), int(n)))
 
     def state_device_ptr(self):
         p, n = C.c_void_p(), C.c_size_t()

@@ -56,6 +56,19 @@ struct sf_solver {
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
+  // sf_step_host_async: copy streams, two staging buffers per direction and
+  // the events that order them with the solver's stream
+  struct HostPipe {
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    float2* in[2] = {nullptr, nullptr};
+    float2* out[2] = {nullptr, nullptr};
+    cudaEvent_t ev_in[2] = {nullptr, nullptr};       // input copied to in[b]
+    cudaEvent_t ev_used[2] = {nullptr, nullptr};     // in[b] taken into the state
+    cudaEvent_t ev_done[2] = {nullptr, nullptr};     // result in out[b]
+    cudaEvent_t ev_drained[2] = {nullptr, nullptr};  // out[b] copied to the host
+    long long k = 0;
+  };
+  HostPipe* pipe = nullptr;
 };
 
 static const double kBeta[3] = {1.0, 25.0 / 8.0, 9.0 / 4.0};     // IMEXRK.h:631
@@ -84,6 +97,21 @@ static void free_all(sf_solver* s) {
                   s->red, s->tw, s->stage_ref};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (sf_solver::HostPipe* P = s->pipe) {
+    if (P->h2d) cudaStreamSynchronize(P->h2d);
+    if (P->d2h) cudaStreamSynchronize(P->d2h);
+    for (int b = 0; b < 2; b++) {
+      if (P->in[b]) cudaFree(P->in[b]);
+      if (P->out[b]) cudaFree(P->out[b]);
+      cudaEvent_t* evs[] = {&P->ev_in[b], &P->ev_used[b], &P->ev_done[b], &P->ev_drained[b]};
+      for (cudaEvent_t* e : evs)
+        if (*e) cudaEventDestroy(*e);
+    }
+    if (P->h2d) cudaStreamDestroy(P->h2d);
+    if (P->d2h) cudaStreamDestroy(P->d2h);
+    delete P;
+    s->pipe = nullptr;
+  }
   if (s->st) cudaStreamDestroy(s->st);
 }
 
@@ -515,6 +543,43 @@ static int step_impl(sf_solver* s, int nsteps, bool linear) {
 }
 
 int sf_step(sf_solver* s, int nsteps) { return step_impl(s, nsteps, false); }
+
+int sf_step_host_async(sf_solver* s, const float* host_in, float* host_out, int nsteps) {
+  if (!s || !host_in || !host_out || nsteps < 0) return fail(SF_EINVAL, "bad argument");
+  const size_t bytes = sizeof(float2) * s->g.nrun * 5 * s->g.fblk;
+  if (!s->pipe) {
+    s->pipe = new sf_solver::HostPipe();
+    sf_solver::HostPipe& P = *s->pipe;
+    CK(cudaStreamCreateWithFlags(&P.h2d, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&P.d2h, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; b++) {
+      CK(cudaMalloc(&P.in[b], bytes));
+      CK(cudaMalloc(&P.out[b], bytes));
+      cudaEvent_t* evs[] = {&P.ev_in[b], &P.ev_used[b], &P.ev_done[b], &P.ev_drained[b]};
+      for (cudaEvent_t* e : evs) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+  }
+  sf_solver::HostPipe& P = *s->pipe;
+  const int b = (int)(P.k & 1);
+  // the input, once the call two back has taken staging buffer b into its state
+  CK(cudaStreamWaitEvent(P.h2d, P.ev_used[b], 0));
+  CK(cudaMemcpyAsync(P.in[b], host_in, bytes, cudaMemcpyHostToDevice, P.h2d));
+  CK(cudaEventRecord(P.ev_in[b], P.h2d));
+  CK(cudaStreamWaitEvent(s->st, P.ev_in[b], 0));
+  CK(cudaMemcpyAsync(s->S[s->cur], P.in[b], bytes, cudaMemcpyDeviceToDevice, s->st));
+  CK(cudaEventRecord(P.ev_used[b], s->st));
+  int rc = step_impl(s, nsteps, false);
+  if (rc != SF_OK) return rc;
+  // the result, once the output copy of the call two back has left buffer b
+  CK(cudaStreamWaitEvent(s->st, P.ev_drained[b], 0));
+  CK(cudaMemcpyAsync(P.out[b], s->S[s->cur], bytes, cudaMemcpyDeviceToDevice, s->st));
+  CK(cudaEventRecord(P.ev_done[b], s->st));
+  CK(cudaStreamWaitEvent(P.d2h, P.ev_done[b], 0));
+  CK(cudaMemcpyAsync(host_out, P.out[b], bytes, cudaMemcpyDeviceToHost, P.d2h));
+  CK(cudaEventRecord(P.ev_drained[b], P.d2h));
+  P.k++;
+  return SF_OK;
+}
 int sf_step_linear(sf_solver* s, int nsteps) { return step_impl(s, nsteps, true); }
 
 int sf_set_base(sf_solver* s, int run, const float* u1, const float* u2, const float* u3, const float* b) {
@@ -730,6 +795,10 @@ int sf_set_tangent(sf_solver* s, int nbase) {
 int sf_synchronize(sf_solver* s) {
   if (!s) return fail(SF_EINVAL, "null solver");
   CK(cudaStreamSynchronize(s->st));
+  if (s->pipe) {
+    CK(cudaStreamSynchronize(s->pipe->h2d));
+    CK(cudaStreamSynchronize(s->pipe->d2h));
+  }
   return SF_OK;
 }
 
