@@ -173,85 +173,7 @@ __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int
   return L;
 }
 
-// One term (a0 F[s] + a1 F[s-1] + a2)(b0 G[s] + b1 G[s+1] + b2) of a product:
-// every product of BuildRHS is one such term and every product of
-// BuildRHSLinear the sum of two.
-// rows are float offsets from the start of the nodal block of shared memory
-struct PTerm {
-  int F, Fm, Gs, Gp;
-  float a0, a1, a2, b0, b1, b2;
-};
-
-__device__ __forceinline__ void term_set(PTerm& T, int F, int Fm, float a0, float a1, float a2, int Gs, int Gp,
-                                         float b0, float b1, float b2) {
-  T.F = F; T.Fm = Fm; T.a0 = a0; T.a1 = a1; T.a2 = a2;
-  T.Gs = Gs; T.Gp = Gp; T.b0 = b0; T.b1 = b1; T.b2 = b2;
-}
-
-// the terms of product p of BuildRHSLinear (IMEXRK.cpp:212-257) at slot s
-// (level t); rows of the nodal fields U1,U2,U3,B (`nr`) and of the base
-// (`br`: U1b+U_, U2b, U3b, Bb)
-__device__ __forceinline__ void prod_terms_linear(int p, int s, int t, int N3, int N1, int NS, const float* zc,
-                                                  PTerm& T0, PTerm& T1) {
-  // the base rows follow the nodal rows in shared memory (x_layout)
-  auto nr = [&](int f, int ss) { return (f * NS + ss) * N1; };
-  auto br = [&](int f, int ss) { return ((4 + f) * NS + ss) * N1; };
-  const bool lo = (t >= 1) && (s >= 1);    // Bar/Tilde rows j >= 1 have a level below
-  const int sm = lo ? s - 1 : s;
-  const float top = (t <= N3 - 2) ? 1.f : 0.f;   // ReinterpolateDirichlet's last row
-  const int sp = (t <= N3 - 2) ? s + 1 : s;
-  const float lof = lo ? 1.f : 0.f;
-  const float tlo = lof * zc[ZC_TILDE_LO * N3 + t], tdi = lof * zc[ZC_TILDE_DI * N3 + t];
-  const float hb = 0.5f * lof;
-  const int z = nr(0, s);   // any valid row for unused terms
-  term_set(T1, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
-  switch (p) {
-    case P_S1: term_set(T0, nr(0, s), z, 2.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f); break;
-    case P_SB1:
-      term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(0, s), z, 1.f, 0.f, 0.f);
-      term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(0, s), z, 1.f, 0.f, 0.f);
-      break;
-    case P_P3:
-      term_set(T0, nr(0, s), nr(0, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
-      term_set(T1, br(0, s), br(0, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-      break;
-    case P_Q1:
-      term_set(T0, nr(0, s), nr(0, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-      term_set(T1, br(0, s), br(0, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-      break;
-    case P_QB:
-      term_set(T0, nr(3, s), nr(3, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-      term_set(T1, br(3, s), br(3, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-      break;
-    case P_P4:   // 2 Dir(U3) Dir(U3b)
-      term_set(T0, nr(2, s), nr(2, sp), 1.f, top, 0.f, br(2, s), br(2, sp), 0.5f, 0.5f * top, 0.f);
-      break;
-    case P_S12:
-      term_set(T0, nr(0, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
-      term_set(T1, br(0, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
-      break;
-    case P_S22: term_set(T0, nr(1, s), z, 2.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f); break;
-    case P_SB2:
-      term_set(T0, nr(3, s), z, 1.f, 0.f, 0.f, br(1, s), z, 1.f, 0.f, 0.f);
-      term_set(T1, br(3, s), z, 1.f, 0.f, 0.f, nr(1, s), z, 1.f, 0.f, 0.f);
-      break;
-    case P_Q2:
-      term_set(T0, nr(1, s), nr(1, sm), hb, hb, 0.f, br(2, s), z, lof, 0.f, 0.f);
-      term_set(T1, br(1, s), br(1, sm), hb, hb, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-      break;
-    case P_P3Y:
-      term_set(T0, nr(1, s), nr(1, sm), tdi, tlo, 0.f, br(2, s), z, lof, 0.f, 0.f);
-      term_set(T1, br(1, s), br(1, sm), tdi, tlo, 0.f, nr(2, s), z, lof, 0.f, 0.f);
-      break;
-    default: term_set(T0, z, z, 0.f, 0.f, 0.f, z, z, 0.f, 0.f, 0.f);
-  }
-}
-
-__device__ __forceinline__ float term_eval(const float* rows, const PTerm& T, int x) {
-  return (T.a0 * rows[T.F + x] + T.a1 * rows[T.Fm + x] + T.a2) * (T.b0 * rows[T.Gs + x] + T.b1 * rows[T.Gp + x] + T.b2);
-}
-
-// ---- BuildRHS products by pair (the nonlinear x pass) ----
+// ---- BuildRHS / BuildRHSLinear products by pair ----
 // Each forward transform carries two real products; a pair kind fixes which
 // two, so the rows each lane reads and the arithmetic are compile-time
 // constants and the two products of a pair share their loads. Products at
@@ -308,13 +230,49 @@ __device__ __forceinline__ float prod_at(const float* nod, int NS, const HalfC& 
   return c.live ? v : 0.f;
 }
 
-template <int P0, int P1, int N1, int E, int G>
-__device__ __forceinline__ void pair_eval(float2 (&x)[E], const float* nod, int NS, const HalfC& c0, const HalfC& c1,
-                                          bool two, int l) {
+// product P of BuildRHSLinear at point n (IMEXRK.cpp:212-257): the
+// derivative of BuildRHS's product about the base, whose rows `bas` hold
+// U1b + U_, U2b, U3b, Bb (so the U_ terms come with the base's u1)
+template <int P, int N1>
+__device__ __forceinline__ float prod_at_lin(const float* nod, const float* bas, int NS, const HalfC& c, int n) {
+  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * N1 + n]; };
+  auto U = [&](int f, int slot) { return bas[(f * NS + slot) * N1 + n]; };
+  float v;
+  if constexpr (P == P_S1) v = (2.f * u(0, c.s)) * U(0, c.s);
+  else if constexpr (P == P_SB1) v = u(3, c.s) * U(0, c.s) + U(3, c.s) * u(0, c.s);
+  else if constexpr (P == P_P3)
+    v = (c.tdi * u(0, c.s) + c.tlo * u(0, c.sm)) * (c.lof * U(2, c.s)) +
+        (c.tdi * U(0, c.s) + c.tlo * U(0, c.sm)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_Q1)
+    v = (c.hb * u(0, c.s) + c.hb * u(0, c.sm)) * (c.lof * U(2, c.s)) +
+        (c.hb * U(0, c.s) + c.hb * U(0, c.sm)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_QB)
+    v = (c.hb * u(3, c.s) + c.hb * u(3, c.sm)) * (c.lof * U(2, c.s)) +
+        (c.hb * U(3, c.s) + c.hb * U(3, c.sm)) * (c.lof * u(2, c.s));
+  else if constexpr (P == P_P4)   // 2 Dir(u3) Dir(U3b)
+    v = (u(2, c.s) + c.top * u(2, c.sp)) * (0.5f * U(2, c.s) + 0.5f * c.top * U(2, c.sp));
+  else if constexpr (P == P_S12) v = u(0, c.s) * U(1, c.s) + U(0, c.s) * u(1, c.s);
+  else if constexpr (P == P_S22) v = (2.f * u(1, c.s)) * U(1, c.s);
+  else if constexpr (P == P_SB2) v = u(3, c.s) * U(1, c.s) + U(3, c.s) * u(1, c.s);
+  else if constexpr (P == P_Q2)
+    v = (c.hb * u(1, c.s) + c.hb * u(1, c.sm)) * (c.lof * U(2, c.s)) +
+        (c.hb * U(1, c.s) + c.hb * U(1, c.sm)) * (c.lof * u(2, c.s));
+  else   // P_P3Y
+    v = (c.tdi * u(1, c.s) + c.tlo * u(1, c.sm)) * (c.lof * U(2, c.s)) +
+        (c.tdi * U(1, c.s) + c.tlo * U(1, c.sm)) * (c.lof * u(2, c.s));
+  return c.live ? v : 0.f;
+}
+
+template <int P0, int P1, int N1, int E, int G, bool LINEAR>
+__device__ __forceinline__ void pair_eval(float2 (&x)[E], const float* nod, const float* bas, int NS, const HalfC& c0,
+                                          const HalfC& c1, bool two, int l) {
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const int n = l + G * e;
-    x[e] = make_float2(prod_at<P0, N1>(nod, NS, c0, n), two ? prod_at<P1, N1>(nod, NS, c1, n) : 0.f);
+    if constexpr (LINEAR)
+      x[e] = make_float2(prod_at_lin<P0, N1>(nod, bas, NS, c0, n), two ? prod_at_lin<P1, N1>(nod, bas, NS, c1, n) : 0.f);
+    else
+      x[e] = make_float2(prod_at<P0, N1>(nod, NS, c0, n), two ? prod_at<P1, N1>(nod, NS, c1, n) : 0.f);
   }
 }
 
@@ -470,117 +428,66 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   // ---- phase B/C: nodal products, forward transforms in pairs (ToModal) ----
   const int nprod = L.nprod;
   const float sc = 0.5f * g.inv_n12;
-  if constexpr (!LINEAR) {
-    const int NT = g.dim3 ? 5 : 3;   // pair kinds at every output level
-    const int nmain = NT * S, nq2 = g.dim3 ? (S + 1) / 2 : 0, ntB = nmain + nq2 + (it == 0 ? 2 : 0);
-    for (int base = 0; base < ntB; base += NGB) {
-      const int task = base + gid;
-      int kind = -1, i = 0;
-      if (task < nmain) {
-        const int q = task / S;
-        kind = q < 2 ? q : (g.dim3 ? q : K_QQB);   // 2D: (S1, SB1), (P3, P4), (Q1, QB)
-        i = task - q * S;
-      } else if (task < nmain + nq2) {
-        kind = K_Q2Q2;
-        i = 2 * (task - nmain);
-      } else if (task < ntB) {
-        kind = task == nmain + nq2 ? K_QQB : K_HALO;
-        i = -1;
-      }
-      int s0 = i + 1, s1 = i + 1, p0 = -1, p1 = -1;
-      switch (kind) {
-        case K_SSB1: p0 = P_S1; p1 = P_SB1; break;
-        case K_P34: p0 = P_P3; p1 = P_P4; break;
-        case K_S122: p0 = P_S12; p1 = P_S22; break;
-        case K_SB2P: p0 = P_SB2; p1 = P_P3Y; break;
-        case K_QQB: p0 = P_Q1; p1 = P_QB; s0 = s1 = i + 2; break;
-        case K_Q2Q2: p0 = P_Q2; p1 = i + 1 < S ? P_Q2 : -1; s0 = i + 2; s1 = i + 3; break;
-        case K_HALO: p0 = P_P4; p1 = g.dim3 ? P_Q2 : -1; s0 = 0; s1 = 1; break;
-        default: break;
-      }
-      const HalfC c0 = half_coeffs(s0, j0, N3, Ub, zc), c1 = half_coeffs(s1, j0, N3, Ub, zc);
-      const bool two = p1 >= 0;
-      float2 x[E];
-      switch (kind) {
-        case K_SSB1: pair_eval<P_S1, P_SB1, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
-        case K_P34: pair_eval<P_P3, P_P4, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
-        case K_S122: pair_eval<P_S12, P_S22, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
-        case K_SB2P: pair_eval<P_SB2, P_P3Y, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
-        case K_QQB: pair_eval<P_Q1, P_QB, N1, E, G>(x, nod, NS, c0, c1, true, l); break;
-        case K_Q2Q2: pair_eval<P_Q2, P_Q2, N1, E, G>(x, nod, NS, c0, c1, two, l); break;
-        case K_HALO: pair_eval<P_P4, P_Q2, N1, E, G>(x, nod, NS, c0, c1, two, l); break;
-        default:
-#pragma unroll
-          for (int e = 0; e < E; e++) x[e] = make_float2(0.f, 0.f);
-      }
-      fft_fwd(x);
-#pragma unroll
-      for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
-      __syncwarp();
-      if (p0 >= 0) {
-        float2* h0 = hat + (size_t)hat_row(p0, s0, S) * K1;
-        float2* h1 = hat + (size_t)hat_row(two ? p1 : p0, s1, S) * K1;
-#pragma unroll
-        for (int q = 0; q < (K1 + G - 1) / G; q++) {
-          const int k = l + q * G;
-          if (k >= K1) break;
-          const float2 zk = buf[k];
-          const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
-          h0[k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);          // (Zk + conj Z_{N-k}) / 2
-          if (two) h1[k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);  // (Zk - conj Z_{N-k}) / (2i)
-        }
-      }
-      __syncwarp();
+  const int NT = g.dim3 ? 5 : 3;   // pair kinds at every output level
+  const int nmain = NT * S, nq2 = g.dim3 ? (S + 1) / 2 : 0, ntB = nmain + nq2 + (it == 0 ? 2 : 0);
+  for (int base = 0; base < ntB; base += NGB) {
+    const int task = base + gid;
+    int kind = -1, i = 0;
+    if (task < nmain) {
+      const int q = task / S;
+      kind = q < 2 ? q : (g.dim3 ? q : K_QQB);   // 2D: (S1, SB1), (P3, P4), (Q1, QB)
+      i = task - q * S;
+    } else if (task < nmain + nq2) {
+      kind = K_Q2Q2;
+      i = 2 * (task - nmain);
+    } else if (task < ntB) {
+      kind = task == nmain + nq2 ? K_QQB : K_HALO;
+      i = -1;
     }
-  } else {
-    int ncar = 0;
-    for (int p = 0; p < nprod; p++) ncar += carried(p) ? 1 : 0;
-    const int nrows = L.nrows - (it > 0 ? ncar : 0);
-    const int ntB = (nrows + 1) / 2;
-    for (int base = 0; base < ntB; base += NGB) {
-      const int task = base + gid;
-      int pp[2], ss[2], row[2];
-      bool live[2];
-      PTerm T[2][2];
+    int s0 = i + 1, s1 = i + 1, p0 = -1, p1 = -1;
+    switch (kind) {
+      case K_SSB1: p0 = P_S1; p1 = P_SB1; break;
+      case K_P34: p0 = P_P3; p1 = P_P4; break;
+      case K_S122: p0 = P_S12; p1 = P_S22; break;
+      case K_SB2P: p0 = P_SB2; p1 = P_P3Y; break;
+      case K_QQB: p0 = P_Q1; p1 = P_QB; s0 = s1 = i + 2; break;
+      case K_Q2Q2: p0 = P_Q2; p1 = i + 1 < S ? P_Q2 : -1; s0 = i + 2; s1 = i + 3; break;
+      case K_HALO: p0 = P_P4; p1 = g.dim3 ? P_Q2 : -1; s0 = 0; s1 = 1; break;
+      default: break;
+    }
+    const HalfC c0 = half_coeffs(s0, j0, N3, Ub, zc), c1 = half_coeffs(s1, j0, N3, Ub, zc);
+    const bool two = p1 >= 0;
+    float2 x[E];
+    switch (kind) {
+      case K_SSB1: pair_eval<P_S1, P_SB1, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, true, l); break;
+      case K_P34: pair_eval<P_P3, P_P4, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, true, l); break;
+      case K_S122: pair_eval<P_S12, P_S22, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, true, l); break;
+      case K_SB2P: pair_eval<P_SB2, P_P3Y, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, true, l); break;
+      case K_QQB: pair_eval<P_Q1, P_QB, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, true, l); break;
+      case K_Q2Q2: pair_eval<P_Q2, P_Q2, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, two, l); break;
+      case K_HALO: pair_eval<P_P4, P_Q2, N1, E, G, LINEAR>(x, nod, bnod, NS, c0, c1, two, l); break;
+      default:
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
-        int r = 2 * task + h;
-        pp[h] = -1; ss[h] = 0; live[h] = false; row[h] = r;
-        if (task < ntB && r < nrows) {
-          for (int p = 0; p < nprod; p++) {
-            int f0, c; prod_slots(p, S, f0, c);
-            const int skip = (it > 0 && carried(p)) ? 1 : 0;
-            if (r < c - skip) { pp[h] = p; ss[h] = f0 + skip + r; break; }
-            r -= c - skip;
-          }
-          if (pp[h] >= 0) row[h] = hat_row(pp[h], ss[h], S);
-          const int t = j0 - 1 + ss[h];
-          live[h] = (pp[h] >= 0) && t >= 0 && t < N3;
-        }
-        prod_terms_linear(live[h] ? pp[h] : -1, ss[h], live[h] ? j0 - 1 + ss[h] : 0, N3, N1, NS, zc, T[h][0], T[h][1]);
-      }
-      float2 x[E];
+        for (int e = 0; e < E; e++) x[e] = make_float2(0.f, 0.f);
+    }
+    fft_fwd(x);
 #pragma unroll
-      for (int e = 0; e < E; e++) {
-        const int n = l + G * e;
-        x[e] = make_float2(term_eval(nod, T[0][0], n) + term_eval(nod, T[0][1], n),
-                           term_eval(nod, T[1][0], n) + term_eval(nod, T[1][1], n));
-      }
-      fft_fwd(x);
-      // natural order in the group's buffer, then split the two real transforms
+    for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
+    __syncwarp();
+    if (p0 >= 0) {
+      float2* h0 = hat + (size_t)hat_row(p0, s0, S) * K1;
+      float2* h1 = hat + (size_t)hat_row(two ? p1 : p0, s1, S) * K1;
 #pragma unroll
-      for (int sl = 0; sl < E; sl++) buf[reg_fft_out_index<N1>(l, sl)] = x[sl];
-      __syncwarp();
-      for (int k = l; k < K1; k += G) {
+      for (int q = 0; q < (K1 + G - 1) / G; q++) {
+        const int k = l + q * G;
+        if (k >= K1) break;
         const float2 zk = buf[k];
         const float2 zc2 = cconj(buf[(N1 - k) & (N1 - 1)]);
-        if (pp[0] >= 0)   // (Zk + conj Z_{N-k}) / 2
-          hat[(size_t)row[0] * K1 + k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);
-        if (pp[1] >= 0)   // (Zk - conj Z_{N-k}) / (2i)
-          hat[(size_t)row[1] * K1 + k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);
+        h0[k] = make_float2((zk.x + zc2.x) * sc, (zk.y + zc2.y) * sc);          // (Zk + conj Z_{N-k}) / 2
+        if (two) h1[k] = make_float2((zk.y - zc2.y) * sc, -(zk.x - zc2.x) * sc);  // (Zk - conj Z_{N-k}) / (2i)
       }
-      __syncwarp();
     }
+    __syncwarp();
   }
   __syncthreads();
 
