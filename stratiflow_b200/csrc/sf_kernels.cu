@@ -156,8 +156,9 @@ __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int
   // input rows of phase A (4 x (S+2) x K1, twice that when the base rows of
   // a tangent-linear batch come along): their own bytes when a block loads
   // the next slab's rows during this slab's work, else the same bytes
-  size_t hat = sizeof(float2) * (size_t)L.nrows * K1,
-         stage = sizeof(float2) * (size_t)(tlm ? 8 : 4) * (S + 2) * K1;
+  auto al16 = [](size_t b) { return (b + 15) & ~(size_t)15; };   // 16-byte aligned regions
+  size_t hat = al16(sizeof(float2) * (size_t)L.nrows * K1),
+         stage = al16(sizeof(float2) * (size_t)(tlm ? 8 : 4) * (S + 2) * K1);
   L.hat_off = off;
   if (prefetch) {
     off += hat;
@@ -281,6 +282,11 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+// 16-byte asynchronous copy (both addresses 16-byte aligned)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
 
 // One block per (`iters` consecutive slabs of S output levels, y row, run).
 // Lane groups of G lanes each run one transform at a time; all groups of the
@@ -353,20 +359,27 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   const int s0 = it == 0 ? 0 : 2;   // nodal slots 0, 1 come from the slab below
   const int NSn = NS - s0;
 
-  if (LINEAR && !tlm) {  // frozen nodal base rows (IMEXRK.h:344-351), U1b + U_ as nnTemp
-    for (int i = threadIdx.x; i < 4 * NS * N1; i += blockDim.x) {
-      int f = i / (NS * N1), r = i - f * NS * N1, s = r / N1, x = r - s * N1;
-      int t = j0 - 1 + s;
-      float v = 0.f;
-      if (t >= 0 && t < N3 && (f != 1 || g.dim3)) {
-        v = a.base[(((size_t)(run * 4 + f) * N3 + t) * g.N2 + y) * N1 + x];
-        if (f == 0) v += Ub[t];
+  if (LINEAR && !tlm) {  // frozen nodal base rows (IMEXRK.h:344-351), one warp per row
+    const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
+    for (int row = threadIdx.x >> 5; row < 4 * NS; row += nw) {
+      const int f = row / NS, t = j0 - 1 + row - f * NS;
+      float* d = bnod + (size_t)row * N1;
+      if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
+        for (int x = lane; x < N1; x += 32) d[x] = 0.f;
+      } else {
+        const float* src = a.base + (((size_t)(run * 4 + f) * N3 + t) * g.N2 + y) * N1;
+        for (int c = lane; c < N1 / 4; c += 32) cp_async16(d + 4 * c, src + 4 * c);
       }
-      bnod[i] = v;
     }
   }
   cp_async_wait_all();
   __syncthreads();
+  if (LINEAR && !tlm) {   // U1b + U_ as nnTemp (phase A writes only the own rows meanwhile)
+    for (int i = threadIdx.x; i < NS * N1; i += blockDim.x) {
+      const int t = j0 - 1 + i / N1;
+      if (t >= 0 && t < N3) bnod[i] += Ub[t];
+    }
+  }
 
   // ---- phase A: inverse transforms of (u1, u3) and (b, u2) (ToNodal) ----
   // (and of the base run's fields for a tangent-linear batch)
