@@ -181,7 +181,7 @@ struct Context {
 class Vec {
  public:
   explicit Vec(Context& c) : c_(&c), s_(new Store(*c.solver, c.M)) {}
-  Vec(const Vec& o) : c_(o.c_), s_(new Store(*o.c_->solver, o.c_->M)), p(o.p), q(o.q) {
+  Vec(const Vec& o) : p(o.p), q(o.q), c_(o.c_), s_(new Store(*o.c_->solver, o.c_->M)) {
     check(sf_vecs_copy_range(o));
   }
   Vec& operator=(const Vec& o) {
