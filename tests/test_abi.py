@@ -53,3 +53,24 @@ def test_package_fails_loudly_without_library(tmp_path):
 def test_library_is_built_for_sm100a():
     from stratiflow_b200 import build
     assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH)
+
+
+def host_functions():
+    src = open(os.path.join(ROOT, "stratiflow_b200", "host", "sf_host.cpp")).read()
+    return sorted(set(re.findall(r"^(?:int|const char\*)\s+(sfh_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_host_library_exports_its_entry_points_and_python_binds_them():
+    """libstratiflow_host.so (the C++ drivers) exports every entry point
+    sf_host.cpp defines, and the Python front end gives each of them its
+    argument types (ctypes would otherwise pass doubles as ints)."""
+    from stratiflow_b200 import build, drivers
+    build.build()
+    names = host_functions()
+    assert {"sfh_newton_fixed", "sfh_arnoldi", "sfh_inverse_iteration", "sfh_critical_point",
+            "sfh_find_hopf", "sfh_linear_evolve"} <= set(names)
+    L = drivers.load_host()
+    for n in names:
+        assert hasattr(L, n), n
+        if n != "sfh_last_error":
+            assert getattr(L, n).argtypes is not None, n
