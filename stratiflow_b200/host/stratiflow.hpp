@@ -1971,6 +1971,51 @@ class HopfNK : public NewtonKrylov {
   Vec A_;
 };
 
+// The GMRES least-squares problem min |beta e_0 - H y| over the columns of the
+// Hessenberg matrix H received so far, kept in QR form by Givens rotations:
+// add() takes column k-1 (rows 0..k) and returns the relative residual of
+// the k-column problem, solve() its minimiser. For H of full column rank
+// this is the minimiser the reference computes by an SVD of H
+// (InverseIteration.cpp:86-104).
+class GivensLS {
+ public:
+  explicit GivensLS(double beta) : beta_(beta), g_(1, beta) {}
+  double add(std::vector<double> h) {
+    const int k = (int)R_.size() + 1;   // h has k + 1 entries
+    for (int j = 0; j < k - 1; j++) {   // the earlier rotations
+      const double a = h[j], b = h[j + 1];
+      h[j] = cs_[j] * a + sn_[j] * b;
+      h[j + 1] = -sn_[j] * a + cs_[j] * b;
+    }
+    const double r = std::hypot(h[k - 1], h[k]);
+    const double c = r > 0 ? h[k - 1] / r : 1.0, sn = r > 0 ? h[k] / r : 0.0;
+    cs_.push_back(c);
+    sn_.push_back(sn);
+    h[k - 1] = r;
+    h[k] = 0;
+    g_.push_back(-sn * g_[k - 1]);
+    g_[k - 1] = c * g_[k - 1];
+    R_.push_back(h);
+    return std::fabs(g_[k]) / beta_;
+  }
+  std::vector<double> solve() const {   // back substitution R y = g
+    const int n = (int)R_.size();
+    std::vector<double> y(n, 0.0);
+    for (int i = n - 1; i >= 0; i--) {
+      double s = g_[i];
+      for (int j = i + 1; j < n; j++) s -= R_[j][i] * y[j];
+      y[i] = R_[i][i] != 0 ? s / R_[i][i] : 0.0;
+    }
+    return y;
+  }
+  double last_pivot() const { return R_.empty() ? 0.0 : R_.back()[R_.size() - 1]; }
+
+ private:
+  double beta_;
+  std::vector<double> g_, cs_, sn_;
+  std::vector<std::vector<double>> R_;   // reduced columns
+};
+
 struct InverseIterationResult {
   std::vector<double> mu;         // |L b| / |b| before each solve (muApprox)
   std::vector<double> residual;   // |L b - muApprox b| with |b| = 1
@@ -2004,9 +2049,7 @@ inline InverseIterationResult InverseIteration(const Vec& about, Vec& b, double 
     q[0]->EnforceBCs();
     const double beta = q[0]->Norm();
     *q[0] *= 1.0 / beta;
-    // Hessenberg columns, reduced by Givens rotations as they arrive
-    std::vector<std::vector<double>> R;
-    std::vector<double> cs, sn, g(1, beta);
+    GivensLS ls(beta);   // the Hessenberg columns, reduced as they arrive
     int used = 0;
     for (int k = 1; k < K; k++) {
       q.emplace_back(new Vec(*q[k - 1]));
@@ -2021,35 +2064,16 @@ inline InverseIterationResult InverseIteration(const Vec& about, Vec& b, double 
       if (h[k] > 0) *q[k] *= 1.0 / h[k];
       q[k]->EnforceBCs();
       used = k;
-      for (int j = 0; j < k - 1; j++) {   // earlier rotations
-        const double a = h[j], bb = h[j + 1];
-        h[j] = cs[j] * a + sn[j] * bb;
-        h[j + 1] = -sn[j] * a + cs[j] * bb;
-      }
-      const double rr = std::hypot(h[k - 1], h[k]);
-      const double cj = rr > 0 ? h[k - 1] / rr : 1.0, sj = rr > 0 ? h[k] / rr : 0.0;
-      cs.push_back(cj);
-      sn.push_back(sj);
-      h[k - 1] = rr;
-      h[k] = 0;
-      g.push_back(-sj * g[k - 1]);
-      g[k - 1] = cj * g[k - 1];
-      R.push_back(h);
-      const double res = std::fabs(g[k]) / beta;
+      const double res = ls.add(h);
       if (verbose() && k % 10 == 0) std::fprintf(stderr, "GMRES STEP %d, RESIDUAL: %.3e\n", k, res);
-      if (res < eps || !(rr > 0)) break;
+      if (res < eps || !(ls.last_pivot() > 0)) break;
     }
-    // back substitution R y = g, then b = sum y_k q_k
-    std::vector<double> y(used, 0.0);
-    for (int i = used - 1; i >= 0; i--) {
-      double s = g[i];
-      for (int j = i + 1; j < used; j++) s -= R[j][i] * y[j];
-      y[i] = R[i][i] != 0 ? s / R[i][i] : 0.0;
-    }
+    out.krylov.push_back(used);
+    if (used == 0) continue;   // no vector to solve with (K < 2): b stays
+    const std::vector<double> y = ls.solve();   // b = sum y_k q_k
     b.Zero();
     for (int k = 0; k < used; k++) b.MulAdd(y[k], *q[k]);
     b *= 1.0 / b.Norm();
-    out.krylov.push_back(used);
   }
   return out;
 }

@@ -86,3 +86,53 @@ def test_eigen_lsq_svd_against_lapack(prog, n, seed):
     assert abs(r - np.linalg.norm(B @ yref - b)) <= 1e-9 * np.linalg.norm(b)
     S = np.sort(np.array([float(v) for v in out[pos + 1 + k:pos + 1 + 2 * k]]))[::-1]
     assert np.allclose(S, np.linalg.svd(B, compute_uv=False), rtol=1e-10)
+
+
+GIVENS = r"""
+#include <cstdio>
+#include <vector>
+#include "stratiflow.hpp"
+using namespace stratiflow;
+int main() {
+  int n;
+  double beta;
+  if (std::scanf("%d %lf", &n, &beta) != 2) return 1;
+  GivensLS ls(beta);
+  for (int k = 1; k <= n; k++) {
+    std::vector<double> h(k + 1);
+    for (auto& a : h) if (std::scanf("%lf", &a) != 1) return 1;
+    std::printf("%.17g\n", ls.add(h));
+  }
+  for (double t : ls.solve()) std::printf("%.17g\n", t);
+  return 0;
+}
+"""
+
+
+def test_givens_least_squares_matches_lstsq():
+    """GivensLS (InverseIteration's GMRES least squares): after each new
+    Hessenberg column the relative residual of min |beta e_0 - H y| and, at
+    the end, the minimiser agree with LAPACK's least squares (which the
+    reference's SVD solve equals for H of full rank) to 1e-10."""
+    d = tempfile.mkdtemp()
+    src, exe = os.path.join(d, "g.cpp"), os.path.join(d, "g")
+    open(src, "w").write(GIVENS)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "stratiflow_b200", "host"),
+                    "-I", os.path.join(ROOT, "include"), src, "-o", exe], check=True)
+    rng = np.random.default_rng(7)
+    n, beta = 24, 1.7
+    H = np.triu(rng.standard_normal((n + 1, n)), -1)   # upper Hessenberg
+    feed = [f"{n} {beta:.17g}"]
+    for k in range(1, n + 1):
+        feed.append(" ".join(f"{v:.17g}" for v in H[:k + 1, k - 1]))
+    out = subprocess.run([exe], input="\n".join(feed), capture_output=True, text=True, check=True).stdout.split()
+    vals = np.array([float(v) for v in out])
+    res, y = vals[:n], vals[n:]
+    e0 = np.zeros(n + 1)
+    e0[0] = beta
+    for k in range(1, n + 1):
+        yk, *_ = np.linalg.lstsq(H[:k + 1, :k], e0[:k + 1], rcond=None)
+        want = np.linalg.norm(H[:k + 1, :k] @ yk - e0[:k + 1]) / beta
+        assert abs(res[k - 1] - want) <= 1e-10 * max(1.0, want), k
+    ywant, *_ = np.linalg.lstsq(H, e0, rcond=None)
+    assert np.linalg.norm(y - ywant) <= 1e-10 * np.linalg.norm(ywant)
