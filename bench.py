@@ -232,7 +232,11 @@ def cpu_baseline(wl, budget_s=20.0):
                       + (f", scaled to the {runs}-run job" if runs > 1 else "")}
 
 
-def dist_setup(args):
+def dist_setup(args, backend="nccl"):
+    """One process per GPU under torchrun (RANK / LOCAL_RANK / WORLD_SIZE /
+    MASTER_* from the environment); a short process-group timeout so ranks
+    that wait for one another end with an error. backend "gloo" (CPU tests of
+    this host logic) leaves the GPUs alone."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -241,11 +245,24 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
         pg = dist
     return ws, rank, local, pg
+
+
+def max_over_ranks(x, dist, device="cuda"):
+    """The largest x over all ranks (every rank gets it); x itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 def run_reference(args, wl, ws, rank):
@@ -345,12 +362,8 @@ def main():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
-    ms = e0.elapsed_time(e1)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     launches = s.launch_count() - n0
-    if dist is not None:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
     value = ws * args.steps / (ms / 1e3)
     clocks = clk.summary()
 
@@ -373,12 +386,7 @@ def main():
             dist.barrier()
         t0 = time.perf_counter()
         body()
-        te = time.perf_counter() - t0
-        if dist is not None:
-            t = torch.tensor([te], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
-        return te
+        return max_over_ranks(time.perf_counter() - t0, dist)
 
     def one_by_one():   # each call copies in, steps and copies out before the next
         for _ in range(n_e2e):
