@@ -183,6 +183,17 @@ int sf_set_xpass_slabs(sf_solver* s, int slabs);
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 
+/* Dissipation rates of one run in the normalisation of IMEXRK::KE / PE
+ * (IMEXRK.h:395-411), FP64 accumulation. The reference has no such
+ * diagnostic; these are the sinks of KE and PE due to the viscous and
+ * diffusive terms of its CrankNicolson (IMEXRK.cpp:75-105):
+ *   eps = (1/Re) sum_i InnerProd(grad u_i, grad u_i)
+ *   chi = Ri/(Re Pr) InnerProd(grad b, grad b)
+ * with the Fourier multipliers for ddx, ddy and the staggered ddz of
+ * Differentiation.cpp:35-61, each component integrated (Integration.h:5-35)
+ * on the levels where it lives. */
+int sf_dissipation(sf_solver* s, int run, double* eps, double* chi);
+
 /* StateVector::Dot (StateVector.h:122-134) between run a of solver sa and
  * run b of solver sb (same grid), FP64 accumulation; Ri of run a weights b */
 int sf_dot(sf_solver* sa, int run_a, sf_solver* sb, int run_b, double* out);
@@ -204,7 +215,8 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len);
  * place, p_out = p_in + pressure_multiplier * q (p_out may equal p_in).
  * It calls no allocator: its working memory is a fixed 2 MiB device array
  * inside this library, which limits it to N3 * plane <= 131072 and
- * N3 <= 1024 (larger grids return SF_EINVAL). The first call on a device
+ * N3 <= 1024, plane = roundup(K1*K2, 16) (256 x 1 x 1024, 512 x 1 x 744 and
+ * 64 x 32 x 320 fit; larger grids return SF_EINVAL). The first call on a device
  * looks that array up (cudaGetSymbolAddress), so make it before any stream
  * capture. Work is queued on `stream` (a cudaStream_t; NULL = legacy default
  * stream) and the call returns without waiting. All calls share the array:

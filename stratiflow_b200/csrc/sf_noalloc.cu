@@ -18,12 +18,13 @@
 // stored per mode, and the grid coefficients are computed on the device from
 // N3 and L3, so no host-to-device copy is needed either.
 //
-// Limits and sharing: at most kNaMaxModeLevels = N3 * plane complex values
-// per call and N3 <= 1024 (a 2D grid up to 512 x 1 x 1024, or small 3D
-// grids); larger grids are rejected with SF_EINVAL. All calls on a device
-// share the one array, which keeps the last call's contents; nothing in it
-// has to start at zero (every value is written before it is read within a
-// call). Calls whose GPU work overlaps — on two streams, or from two threads
+// Limits and sharing: at most kNaMaxModeLevels = N3 * plane = 131072 complex
+// values per call and N3 <= 1024, where plane = roundup(K1*K2, 16) is the
+// kept modes of one level (a 2D grid of 256 x 1 x 1024 fits, as do
+// 512 x 1 x 744 and the 3D grid 64 x 32 x 320); larger grids are rejected
+// with SF_EINVAL. All calls on a device share the one array, which keeps the
+// last call's contents; nothing in it has to start at zero (every value is
+// written before it is read within a call). Calls whose GPU work overlaps — on two streams, or from two threads
 // — race on that array and must be serialised by the caller.
 
 #include <cuda_runtime.h>
@@ -124,7 +125,8 @@ __global__ void __launch_bounds__(128) k_na_proj(int N3, int K1, int Ky, int K2,
   const double kyd = dim3 ? kyint * (2 * 3.141592653589793238462) / L2 : 0.0;
   const double kk = -(kxd * kxd) + -(kyd * kyd);
   const float sc = c == 0 ? -1.f : 1.f;
-  float* Dst = reinterpret_cast<float*>(scratch) + c;                  // D_j component c
+  // D_j of this mode and component: [j][2*Pp] floats, mode m at 2m + c
+  float* Dst = reinterpret_cast<float*>(scratch) + 2 * (size_t)m + c;
   float* Cst = reinterpret_cast<float*>(scratch + kNaDBytes);         // C_j
   const double* coef = reinterpret_cast<const double*>(scratch + kNaDBytes + kNaCBytes);
   const size_t s2 = 2 * (size_t)Pp;
