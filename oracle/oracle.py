@@ -54,6 +54,7 @@ def lib():
             ("sfo_step_linear", [vp, i]), ("sfo_remove_divergence", [vp, d]),
             ("sfo_populate_nodal", [vp]), ("sfo_filter_all", [vp]),
             ("sfo_set_base", [vp, dp, dp, dp, dp]), ("sfo_energy", [vp, dp, dp]),
+            ("sfo_dissipation", [vp, dp, dp]),
             ("sfo_to_nodal", [vp, dp, dp]), ("sfo_to_modal", [vp, dp, dp]),
             ("sfo_make_ic", [vp, C.c_uint64, d, i, i, i]), ("sfo_set_threads", [i]),
             ("sfo_step_adjoint", [vp, dp, dp]),
@@ -180,6 +181,13 @@ class Oracle:
         ke, pe = C.c_double(), C.c_double()
         lib().sfo_energy(self.h, C.byref(ke), C.byref(pe))
         return ke.value, pe.value
+
+    def dissipation(self):
+        """(eps, chi): (1/Re) sum_i InnerProd(grad u_i, grad u_i) and
+        Ri/(Re Pr) InnerProd(grad b, grad b), the sinks of KE and PE."""
+        e, c = C.c_double(), C.c_double()
+        lib().sfo_dissipation(self.h, C.byref(e), C.byref(c))
+        return e.value, c.value
 
     def to_nodal(self, modal):
         a = np.ascontiguousarray(np.asarray(modal, dtype=np.complex128).reshape(self.modal_shape))

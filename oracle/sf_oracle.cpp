@@ -902,6 +902,40 @@ struct Solver {
   }
   T PE() const { return Ri * T(0.5) * inner_prod(b, b, Neumann); }  // IMEXRK.h:408-411
 
+  // Dissipation rates in the normalisation of KE and PE (the reference has no
+  // such diagnostic; it is the sink of KE and PE that the viscous and
+  // diffusive terms of CrankNicolson, IMEXRK.cpp:75-105, produce):
+  //   eps = (1/Re) sum_i InnerProd(grad u_i, grad u_i)
+  //   chi = Ri/(Re Pr) InnerProd(grad b, grad b)
+  // with ddx, ddy the Fourier multipliers (Differentiation.cpp:134-160) and
+  // ddz the staggered bidiagonal operators (Differentiation.cpp:35-61), each
+  // gradient component integrated by InnerProd at the location it lives on.
+  T grad_sq(const std::vector<C>& f, BC bc) const {
+    std::vector<C> d(f.size(), C(0));
+    T s = 0;
+    for (int dir = 0; dir < 3; dir++) {
+      if (dir == 1 && !dim3) continue;
+      for (int n2 = 0; n2 < N2; n2++)
+        for (int n1 = 0; n1 < M1; n1++) {
+          const size_t o = midx(n1, n2);
+          for (int j = 0; j < N3; j++) {
+            if (dir == 0) d[o + j] = C(0, kx[n1]) * f[o + j];
+            else if (dir == 1) d[o + j] = C(0, ky[n2]) * f[o + j];
+            else d[o + j] = (bc == Neumann) ? DzND(&f[o], j) : DzDN(&f[o], j);
+          }
+        }
+      const BC at = (dir == 2) ? (bc == Neumann ? Dirichlet : Neumann) : bc;
+      s += inner_prod(d, d, at);
+    }
+    return s;
+  }
+  void dissipation(T& eps, T& chi) const {
+    T g = grad_sq(u1, Neumann) + grad_sq(u3, Dirichlet);
+    if (dim3) g += grad_sq(u2, Neumann);
+    eps = g / Re;
+    chi = Ri / (Re * Pr) * grad_sq(b, Neumann);
+  }
+
   // Nodal1D::SetValue for a Neumann profile (Field.h:661-682)
   void set_background(const double* U) {
     for (int j = 0; j < N3; j++) Ubar[j] = T(U[j]);
@@ -1139,6 +1173,16 @@ void sfo_set_base(void* hv, const double* u1, const double* u2, const double* u3
 void sfo_energy(void* hv, double* ke, double* pe) {
   auto* h = (Handle*)hv;
   DISPATCH(h, { *ke = double(S->KE()); *pe = double(S->PE()); });
+}
+
+void sfo_dissipation(void* hv, double* eps, double* chi) {
+  auto* h = (Handle*)hv;
+  DISPATCH(h, {
+    decltype(S->Ri) e, c;
+    S->dissipation(e, c);
+    *eps = double(e);
+    *chi = double(c);
+  });
 }
 
 // modal fields -> nodal and back (Field.h:734-769, 965-994) on a single

@@ -28,7 +28,7 @@ EXPORTS = [
     "sf_create", "sf_destroy", "sf_last_error", "sf_set_dt", "sf_set_ri", "sf_set_background",
     "sf_set_field", "sf_get_field", "sf_set_state_kept", "sf_get_state_kept", "sf_step_host_async", "sf_state_device",
     "sf_set_state_device", "sf_prepare", "sf_remove_divergence", "sf_step", "sf_set_base",
-    "sf_step_linear", "sf_energy", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
+    "sf_step_linear", "sf_energy", "sf_dissipation", "sf_dot", "sf_synchronize", "sf_stream", "sf_launch_count",
     "sf_profile_step", "sf_profile_names", "sf_remove_divergence_noalloc",
     "sf_vecs_create", "sf_vecs_destroy", "sf_vecs_count", "sf_vecs_device", "sf_vecs_from_run", "sf_vecs_to_run",
     "sf_vecs_copy", "sf_vecs_set_host", "sf_vecs_get_host", "sf_vecs_axpy", "sf_vecs_lincomb", "sf_vecs_scale",
@@ -77,7 +77,7 @@ def load_library(path: str | None = None):
         "sf_state_device": [vp, C.POINTER(vp), C.POINTER(C.c_size_t)], "sf_set_state_device": [vp, vp],
         "sf_prepare": [vp], "sf_remove_divergence": [vp, d], "sf_step": [vp, i],
         "sf_set_base": [vp, i, fp, fp, fp, fp], "sf_step_linear": [vp, i],
-        "sf_energy": [vp, i, dp, dp], "sf_dot": [vp, i, vp, i, dp], "sf_synchronize": [vp],
+        "sf_energy": [vp, i, dp, dp], "sf_dissipation": [vp, i, dp, dp], "sf_dot": [vp, i, vp, i, dp], "sf_synchronize": [vp],
         "sf_stream": [vp, C.POINTER(vp)], "sf_launch_count": [vp, C.POINTER(C.c_longlong)],
         "sf_profile_step": [vp, i, i, i, dp, C.POINTER(i)], "sf_profile_names": [vp, C.c_char_p, C.c_size_t],
         "sf_remove_divergence_noalloc": [C.POINTER(_Grid), C.POINTER(_Flow), d, vp, vp, vp, vp, vp, vp],
@@ -375,6 +375,14 @@ class IMEXRK:
         ke, pe = C.c_double(), C.c_double()
         _check(load_library().sf_energy(self._h, int(run), C.byref(ke), C.byref(pe)))
         return ke.value, pe.value
+
+    def dissipation(self, run=0):
+        """(eps, chi): the viscous and diffusive sinks of KE and PE of one run,
+        (1/Re) sum_i InnerProd(grad u_i, grad u_i) and
+        Ri/(Re Pr) InnerProd(grad b, grad b), FP64 accumulation."""
+        e, c = C.c_double(), C.c_double()
+        _check(load_library().sf_dissipation(self._h, int(run), C.byref(e), C.byref(c)))
+        return e.value, c.value
 
     def KE(self, run=0):
         return self.energy(run)[0]

@@ -50,14 +50,29 @@ def build_host(force: bool = False) -> str:
     return HOST_LIB
 
 
+OBJ = os.path.join(HERE, "..", "_build", "obj")
+
+
+def _compile(src: str, verbose: bool) -> str:
+    obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
+    cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-c", "-Xcompiler", "-fPIC",
+           "--expt-relaxed-constexpr", "-o", obj, src]
+    if verbose:
+        cmd += ["-Xptxas", "-v"]
+    subprocess.check_call(cmd)
+    return obj
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every translation unit (in parallel; one object per source
+    under _build/) and link them into the package's shared library."""
     if force or needs_build():
-        cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
-               "--expt-relaxed-constexpr", "-o", LIB]
-        if verbose:
-            cmd += ["-Xptxas", "-v"]
-        cmd += [os.path.join(CSRC, s) for s in SOURCES]
-        subprocess.check_call(cmd)
+        from concurrent.futures import ThreadPoolExecutor
+        os.makedirs(OBJ, exist_ok=True)
+        srcs = [os.path.join(CSRC, s) for s in SOURCES]
+        with ThreadPoolExecutor(max_workers=len(srcs)) as ex:
+            objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
+        subprocess.check_call([NVCC, *ARCH, "-shared", "-o", LIB, *objs])
     build_host(force)
     return LIB
 

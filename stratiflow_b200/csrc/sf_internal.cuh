@@ -101,6 +101,8 @@ int launch_gather_ref(const Geo& g, const float2* ref, float2* kept, cudaStream_
 int launch_scatter_ref(const Geo& g, const float2* kept, float2* ref, cudaStream_t st);
 int launch_energy(const Geo& g, const float2* Sa, const float2* Sb, int nrun_pairs,
                   const float* zc, const float* Ri, double* out, cudaStream_t st);
+int launch_grad_sq(const Geo& g, const float2* S, int nruns, const float* zc, const double* kxd, const double* kyd,
+                   double* out, cudaStream_t st);
 int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* base_out,
                       const float2* tw, float* scratch_mixed, cudaStream_t st);
 

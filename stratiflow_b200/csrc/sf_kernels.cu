@@ -1070,6 +1070,51 @@ __global__ void k_inner(Geo g, const float2* __restrict__ Sa, const float2* __re
   }
 }
 
+// The squared-gradient integrals of the dissipation rates (sf_dissipation),
+// InnerProd (Integration.h:282-311) of each gradient component at the
+// location it lives on, in FP64: per level j the sum over kept modes of
+// w_m [ (kx^2 + ky^2) |a_j|^2 wz(j) + |vertical difference|^2 / dz ], with
+//   u1, u2, b (Neumann): ddz lands on Dirichlet rows, (a_j - a_{j-1}) / DY_j,
+//                        integrated over rows 2..N3-2 with weights DY_j;
+//   u3 (Dirichlet):      ddz lands on Neumann rows, (a_{j+1} - a_j) / DYF_j,
+//                        integrated over rows 1..N3-2 with weights DYF_j
+// (Differentiation.cpp:35-61, Integration.h:5-35). out[run*4 + f] accumulates.
+__global__ void k_grad_sq(Geo g, const float2* __restrict__ S, const float* __restrict__ zc,
+                          const double* __restrict__ kxd, const double* __restrict__ kyd, double* out) {
+  const int j = blockIdx.x, run = blockIdx.y, f = blockIdx.z;
+  const int N3 = g.N3;
+  const bool dir = f == 2;
+  const float2* a = S + ((size_t)(run * 5 + f) * N3 + j) * g.Pp;
+  const double wz = (double)zc[(dir ? ZC_WZD : ZC_WZN) * N3 + j];
+  int jn = -1;
+  double iv = 0.0;
+  if (!dir && j >= 2 && j <= N3 - 2) { jn = j - 1; iv = (double)zc[ZC_DND_DI * N3 + j]; }   // 1/DY_j
+  if (dir && j >= 1 && j <= N3 - 2) { jn = j + 1; iv = (double)zc[ZC_DDN_UP * N3 + j]; }   // 1/DYF_j
+  const float2* an = S + ((size_t)(run * 5 + f) * N3 + (jn >= 0 ? jn : j)) * g.Pp;
+  double s = 0.0;
+  for (int m = threadIdx.x; m < g.P; m += blockDim.x) {
+    const int q = m / g.K1, j1 = m - q * g.K1;
+    const double kk = kxd[j1] * kxd[j1] + (g.dim3 ? kyd[q] * kyd[q] : 0.0);
+    const float2 x = a[m];
+    double v = kk * ((double)x.x * x.x + (double)x.y * x.y) * wz;
+    if (jn >= 0) {
+      const float2 y = an[m];
+      const double dx = (double)x.x - y.x, dy = (double)x.y - y.y;
+      v += (dx * dx + dy * dy) * iv;
+    }
+    s += (m == 0) ? v : 2.0 * v;
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
+    if (t != 0.0) atomicAdd(out + run * 4 + f, t);
+  }
+}
+
 // ======================================================== launchers ====
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
@@ -1280,6 +1325,12 @@ int launch_gather_ref(const Geo& g, const float2* ref, float2* kept, cudaStream_
 
 int launch_scatter_ref(const Geo& g, const float2* kept, float2* ref, cudaStream_t st) {
   k_scatter_ref<<<dim3(cdiv(g.P, 32), cdiv(g.N3, 32)), dim3(32, 8), 0, st>>>(g, kept, ref);
+  return 1;
+}
+
+int launch_grad_sq(const Geo& g, const float2* S, int nruns, const float* zc, const double* kxd, const double* kyd,
+                   double* out, cudaStream_t st) {
+  k_grad_sq<<<dim3(g.N3, nruns, 4), 256, 0, st>>>(g, S, zc, kxd, kyd, out);
   return 1;
 }
 

@@ -657,6 +657,23 @@ int sf_energy(sf_solver* s, int run, double* ke, double* pe) {
   return SF_OK;
 }
 
+int sf_dissipation(sf_solver* s, int run, double* eps, double* chi) {
+  if (!s || run < 0 || run >= s->g.nrun) return fail(SF_EINVAL, "bad argument");
+  const Geo& g = s->g;
+  CK(cudaMemsetAsync(s->red, 0, sizeof(double) * 4, s->st));
+  const float2* st = s->S[s->cur] + (size_t)run * 5 * g.fblk;
+  s->launches += launch_grad_sq(g, st, 1, s->zc, s->kxd, s->kyd, s->red, s->st);
+  CK(cudaGetLastError());
+  double h[4];
+  CK(cudaMemcpyAsync(h, s->red, sizeof(h), cudaMemcpyDeviceToHost, s->st));
+  CK(cudaStreamSynchronize(s->st));
+  double gu = h[0] + h[2];
+  if (g.dim3) gu += h[1];
+  if (eps) *eps = gu / s->Re;
+  if (chi) *chi = (double)s->hRi[run] / (s->Re * s->Pr) * h[3];
+  return SF_OK;
+}
+
 int sf_dot(sf_solver* sa, int ra, sf_solver* sb, int rb, double* out) {
   if (!sa || !sb || !out || ra < 0 || ra >= sa->g.nrun || rb < 0 || rb >= sb->g.nrun)
     return fail(SF_EINVAL, "bad argument");

@@ -51,3 +51,17 @@ def rel_l2(a, b):
     b = np.asarray(b, dtype=np.complex128)
     n = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / (n if n > 0 else 1.0))
+
+
+# measured relative L2 errors of the parity tests, by case; written as JSON to
+# the path in SF_PARITY_TABLE at the end of the session (tests/conftest.py)
+PARITY_TABLE: dict = {}
+
+
+def record_parity(case: str, errs: dict, bounds: dict | None = None):
+    """errs: {(oracle precision, field): relative L2}."""
+    row = PARITY_TABLE.setdefault(case, {})
+    for (prec, f), v in errs.items():
+        row[f"{f} vs FP{prec}"] = float(v)
+        if bounds is not None:
+            row[f"{f} vs FP{prec} bound"] = float(bounds[(prec, f)])

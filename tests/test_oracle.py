@@ -150,3 +150,57 @@ def test_grid_helpers_match_oracle():
     o = O.Oracle(32, 1, 64, 1.0, 1.0, 10.0, 1000, 0.1, 1.0, 0.01, prec=64)
     assert np.allclose(grid.vertical_points(10.0, 64)[1:], o.grid("z")[1:], rtol=1e-14)
     assert np.allclose(grid.vertical_points_fractional(10.0, 64), o.grid("zf"), rtol=1e-14)
+
+
+@pytest.mark.parametrize("name", ["kh2d", "shear3d_small"])
+def test_dissipation_matches_numpy_restatement(name):
+    """The oracle's dissipation rates equal a numpy restatement written from
+    the definitions: per field, sum over modes with the InnerProd weights
+    (1 for (0,0), 2 otherwise; Integration.h:282-311) of (kx^2 + ky^2) |f|^2
+    at the field's own quadrature rows, plus the squared staggered difference
+    ddz f (Differentiation.cpp:35-61) at the other grid's quadrature rows
+    (Integration.h:5-35)."""
+    from stratiflow_b200.grid import vertical_points, vertical_points_fractional
+    cfg = CONFIGS[name]
+    st = make_ic(cfg, seed=5)
+    st["b"] = 0.7 * st["u1"] + 0.2j * st["u3"]   # a non-zero buoyancy field
+    o = make_oracle(cfg, 64)
+    o.set_state(st)
+    eps, chi = o.dissipation()
+    N1, N2, N3 = cfg["N1"], cfg["N2"], cfg["N3"]
+    z = vertical_points(cfg["L3"], N3)
+    zf = vertical_points_fractional(cfg["L3"], N3)
+    DY = np.zeros(N3); DY[1:] = zf[1:] - zf[:-1]
+    DYF = np.zeros(N3); DYF[1:N3 - 1] = z[2:] - z[1:N3 - 1]
+
+    def kint(n):
+        if n == 1:
+            return np.zeros(1)
+        return np.array(list(range(n // 3 + 1)) + [0] * (n - 2 * (n // 3) - 1) + list(range(-(n // 3), 0)),
+                        dtype=float)
+    kx = kint(N1)[:N1 // 2 + 1] * 2 * np.pi / cfg["L1"]
+    ky = kint(N2) * 2 * np.pi / cfg["L2"] if N2 > 1 else np.zeros(1)
+    w = np.full((N2, N1 // 2 + 1), 2.0)
+    w[0, 0] = 1.0
+    k2 = (ky[:, None] ** 2 + kx[None, :] ** 2)[:, :, None]
+
+    def grad_sq(f, neumann):
+        f = np.asarray(f, dtype=np.complex128)
+        a2 = np.abs(f) ** 2
+        if neumann:
+            hz = np.zeros(N3); hz[1:N3 - 1] = DYF[1:N3 - 1]          # Neumann rows 1..N3-2
+            d = np.zeros_like(f); d[:, :, 2:] = (f[:, :, 2:] - f[:, :, 1:-1]) / DY[2:]
+            vz = np.zeros(N3); vz[2:N3 - 1] = DY[2:N3 - 1]           # Dirichlet rows 2..N3-2
+        else:
+            hz = np.zeros(N3); hz[2:N3 - 1] = DY[2:N3 - 1]
+            d = np.zeros_like(f)
+            d[:, :, 1:N3 - 1] = (f[:, :, 2:] - f[:, :, 1:N3 - 1]) / DYF[1:N3 - 1]
+            vz = np.zeros(N3); vz[1:N3 - 1] = DYF[1:N3 - 1]
+        return float(np.sum(w[:, :, None] * (k2 * a2 * hz + np.abs(d) ** 2 * vz)))
+
+    g = grad_sq(st["u1"], True) + grad_sq(st["u3"], False)
+    if N2 > 1:
+        g += grad_sq(st["u2"], True)
+    assert abs(eps - g / cfg["Re"]) <= 1e-12 * abs(eps)
+    c = cfg["Ri"] / (cfg["Re"] * cfg["Pr"]) * grad_sq(st["b"], True)
+    assert abs(chi - c) <= 1e-12 * abs(chi)
