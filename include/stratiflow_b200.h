@@ -180,6 +180,18 @@ int sf_get_runs(sf_solver* s, int* nrun);
  * size). The results do not depend on it. */
 int sf_set_xpass_slabs(sf_solver* s, int slabs);
 
+/* Launch tuning of the 3D x-y pass (no counterpart in the reference): the
+ * number of level bands (1..8) whose y transforms run on side streams beside
+ * the x passes of the neighbouring bands; 1 runs the three kernels one after
+ * the other over all levels. The results do not depend on it. */
+int sf_set_xy_bands(sf_solver* s, int bands);
+
+/* Launch tuning of the z solves (no counterpart in the reference): the
+ * number of z-chunks one block splits each Thomas system into, 8 or 16 (0:
+ * chosen from the grid size). The results depend on it only through
+ * rounding (the chunked solve reassociates the recurrence). */
+int sf_set_z_chunks(sf_solver* s, int chunks);
+
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 
@@ -224,6 +236,34 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len);
 int sf_remove_divergence_noalloc(const sf_grid* grid, const sf_flow* flow, double pressure_multiplier,
                                  void* u1, void* u2, void* u3, const void* p_in, void* p_out,
                                  void* stream);
+
+/* ---- ensembles of 2D runs on different grids (no counterpart in the
+ * reference, whose grid is a compile-time constant, Parameters.h:42-43, held
+ * by one static solver, StateVector.h:546) ----
+ * nrun independent 2D runs, run r on grids[r] (N2 = 1; the nrun field is
+ * ignored) with flows[r] and time step dt[r]. Each run is a member solver
+ * (sf_ensemble_member) that takes every single-solver call: sf_set_ri,
+ * sf_set_background, sf_set_field / sf_get_field, sf_prepare, sf_energy, ...
+ * sf_ensemble_step advances every member by nsteps IMEXRK::TimeStep
+ * (IMEXRK.cpp:8-24) with one x-pass launch and one z-solve launch per RK stage
+ * over all members' work items (one CUDA graph per step); it waits for the
+ * members' own queued work first and returns without waiting for the steps:
+ * call sf_ensemble_synchronize before using a member again. Members must not
+ * be stepped on their own in between (sf_ensemble_step then reports
+ * SF_ESTATE if their state parities differ). The member handles belong to
+ * the ensemble: sf_ensemble_destroy frees them. */
+typedef struct sf_ensemble sf_ensemble;
+int sf_ensemble_create(int nrun, const sf_grid* grids, const sf_flow* flows, const double* dt, int device,
+                       sf_ensemble** out);
+int sf_ensemble_destroy(sf_ensemble* e);
+int sf_ensemble_member(sf_ensemble* e, int run, sf_solver** s);
+int sf_ensemble_step(sf_ensemble* e, int nsteps);
+int sf_ensemble_synchronize(sf_ensemble* e);
+int sf_ensemble_launch_count(sf_ensemble* e, long long* count);
+int sf_ensemble_stream(sf_ensemble* e, void** stream);
+/* nsteps steps run eagerly with CUDA events around every launch: the average
+ * milliseconds of one x-pass launch and of one z-solve launch (all members) */
+int sf_ensemble_profile(sf_ensemble* e, int nsteps, double* ms_x, double* ms_z);
 
 /* ---- device state vectors (StateVector algebra, StateVector.h:40-149) ----
  * A store holds nvec states of one grid on the device, each in the kept

@@ -36,7 +36,9 @@ EXPORTS = [
     "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
-    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_base_device",
+    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_xy_bands", "sf_set_z_chunks",
+    "sf_ensemble_create", "sf_ensemble_destroy", "sf_ensemble_member", "sf_ensemble_step",
+    "sf_ensemble_synchronize", "sf_ensemble_launch_count", "sf_ensemble_stream", "sf_ensemble_profile", "sf_set_base_device",
     "sf_get_nodal", "sf_set_nodal", "sf_velocity_maxima", "sf_cfl", "sf_get_dt", "sf_get_runs", "sf_step_adjoint",
 ]
 
@@ -94,10 +96,14 @@ def load_library(path: str | None = None):
         "sf_net_set_params": [vp, fp], "sf_net_forward": [vp, fp, i, fp], "sf_net_set_data": [vp, fp, fp, i],
         "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
         "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
-        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_base_device": [vp, i, vp],
+        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_xy_bands": [vp, i], "sf_set_z_chunks": [vp, i], "sf_set_base_device": [vp, i, vp],
         "sf_get_nodal": [vp, i, i, fp], "sf_set_nodal": [vp, i, i, fp], "sf_velocity_maxima": [vp, i, dp],
         "sf_cfl": [vp, i, dp], "sf_get_dt": [vp, dp], "sf_get_runs": [vp, C.POINTER(i)],
         "sf_step_adjoint": [vp, vp, vp],
+        "sf_ensemble_create": [i, C.POINTER(_Grid), C.POINTER(_Flow), dp, i, C.POINTER(vp)],
+        "sf_ensemble_destroy": [vp], "sf_ensemble_member": [vp, i, C.POINTER(vp)], "sf_ensemble_step": [vp, i],
+        "sf_ensemble_synchronize": [vp], "sf_ensemble_launch_count": [vp, C.POINTER(C.c_longlong)],
+        "sf_ensemble_stream": [vp, C.POINTER(vp)], "sf_ensemble_profile": [vp, i, dp, dp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)
@@ -127,6 +133,7 @@ class IMEXRK:
     def __init__(self, N1, N2, N3, L1, L2, L3, Re, Pr, dt, nrun=1, device=0):
         L = load_library()
         self.N1, self.N2, self.N3, self.nrun = int(N1), int(N2), int(N3), int(nrun)
+        self.device = int(device)
         self.M1 = self.N1 // 2 + 1
         self.L1, self.L2, self.L3, self.Re, self.Pr = float(L1), float(L2), float(L3), float(Re), float(Pr)
         self.deltaT = float(dt)
@@ -141,10 +148,30 @@ class IMEXRK:
         self.plane = (self.K1 * self.K2 + 15) // 16 * 16
         self.Ri = np.zeros(self.nrun)
 
+    @classmethod
+    def _member(cls, handle, N1, N2, N3, L1, L2, L3, Re, Pr, dt, device=0):
+        """A view of a solver owned by something else (an Ensemble member):
+        every method works, close() does not destroy it."""
+        self = cls.__new__(cls)
+        self.N1, self.N2, self.N3, self.nrun = int(N1), int(N2), int(N3), 1
+        self.device = int(device)
+        self.M1 = self.N1 // 2 + 1
+        self.L1, self.L2, self.L3, self.Re, self.Pr = float(L1), float(L2), float(L3), float(Re), float(Pr)
+        self.deltaT = float(dt)
+        self._h = handle
+        self._owned = False
+        self.dim3 = self.N2 > 1
+        self.K1 = self.N1 // 3
+        self.K2 = 2 * (self.N2 // 3) - 1 if self.dim3 else 1
+        self.plane = (self.K1 * self.K2 + 15) // 16 * 16
+        self.Ri = np.zeros(1)
+        return self
+
     # ---- lifetime ----
     def close(self):
         if getattr(self, "_h", None):
-            load_library().sf_destroy(self._h)
+            if getattr(self, "_owned", True):
+                load_library().sf_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -362,6 +389,23 @@ class IMEXRK:
         """Slabs per x-pass block (0: automatic); a launch setting only."""
         _check(load_library().sf_set_xpass_slabs(self._h, int(slabs)))
 
+    def set_xy_bands(self, bands):
+        """Level bands of the 3D x-y pass (1..8; 1: no side streams); a launch
+        setting only."""
+        _check(load_library().sf_set_xy_bands(self._h, int(bands)))
+
+    def autotune(self, mode="step", steps=8, use_cache=True):
+        """Pick this grid's launch settings by timing candidates on the device
+        (stratiflow_b200.autotune; FFTW_PATIENT's role in the reference,
+        Field.h:719-730); cached per device and grid. Returns the settings."""
+        from . import autotune
+        return autotune.tune(self, mode=mode, steps=steps, use_cache=use_cache)[0]
+
+    def set_z_chunks(self, chunks):
+        """z chunks per block of the z solves (0: automatic, 8 or 16); a
+        launch setting (the results change only by rounding)."""
+        _check(load_library().sf_set_z_chunks(self._h, int(chunks)))
+
     def set_tangent(self, nbase):
         """Runs >= nbase advance linearised about the live run (r - nbase) % nbase."""
         _check(load_library().sf_set_tangent(self._h, int(nbase)))
@@ -420,6 +464,70 @@ class IMEXRK:
         n = C.c_longlong()
         _check(load_library().sf_launch_count(self._h, C.byref(n)))
         return n.value
+
+
+class Ensemble:
+    """Independent 2D runs on grids of different sizes stepped together
+    (sf_ensemble_*): one x-pass launch and one z-solve launch per RK stage
+    over every run's work items, one CUDA graph per step. grids is a list of
+    (N1, N3); flows a list of (L1, L3, Re, Pr) or one tuple for all; dt one
+    value or a list. members[r] is an IMEXRK view of run r (set_ri,
+    SetBackground, set_state, Prepare, get_field, energy, ...)."""
+
+    def __init__(self, grids, flows, dt, device=0):
+        L = load_library()
+        R = len(grids)
+        flows = list(flows) if isinstance(flows, (list, np.ndarray)) and len(flows) == R and \
+            not np.isscalar(flows[0]) else [flows] * R
+        dts = np.broadcast_to(np.asarray(dt, dtype=np.float64), (R,)).copy()
+        g = (_Grid * R)(*[_Grid(int(n1), 1, int(n3), 1) for n1, n3 in grids])
+        f = (_Flow * R)(*[_Flow(float(l1), float(l1) / 2, float(l3), float(re), float(pr))
+                          for l1, l3, re, pr in flows])
+        h = C.c_void_p()
+        _check(L.sf_ensemble_create(R, g, f, dts.ctypes.data_as(C.POINTER(C.c_double)), int(device), C.byref(h)))
+        self._h = h
+        self.members = []
+        for r, ((n1, n3), (l1, l3, re, pr)) in enumerate(zip(grids, flows)):
+            m = C.c_void_p()
+            _check(L.sf_ensemble_member(self._h, r, C.byref(m)))
+            self.members.append(IMEXRK._member(m, n1, 1, n3, l1, l1 / 2, l3, re, pr, dts[r], device))
+
+    def step(self, n=1):
+        """n x IMEXRK::TimeStep of every run; asynchronous."""
+        _check(load_library().sf_ensemble_step(self._h, int(n)))
+
+    def synchronize(self):
+        _check(load_library().sf_ensemble_synchronize(self._h))
+
+    def stream(self):
+        p = C.c_void_p()
+        _check(load_library().sf_ensemble_stream(self._h, C.byref(p)))
+        return p.value
+
+    def launch_count(self):
+        n = C.c_longlong()
+        _check(load_library().sf_ensemble_launch_count(self._h, C.byref(n)))
+        return n.value
+
+    def profile(self, nsteps=3):
+        """(ms of one x-pass launch, ms of one z-solve launch), all members,
+        timed eagerly with CUDA events; advances every run nsteps steps."""
+        a, b = C.c_double(), C.c_double()
+        _check(load_library().sf_ensemble_profile(self._h, int(nsteps), C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m._h = None
+            load_library().sf_ensemble_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Vecs:

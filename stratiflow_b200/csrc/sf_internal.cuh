@@ -77,12 +77,36 @@ struct StageArgs {
   float2* amix;         // 3D adjoint step: 12 y-transformed fields [nrun][12][N3][N2][K1]
   float adj_invK;       // adjoint step: 1/K of the mixing objective (IMEXRK.h:487)
   float h, hz, hb, cv, cb, pm;
+  // level band of one launch of the y transforms (levels lvl0 .. lvl0+nlvl-1;
+  // nlvl = 0: all) and level columns of one x-pass launch (xcol0 .. +xcols-1;
+  // xcols = 0: all), for the banded 3D x-y pass
+  int lvl0, nlvl, xcol0, xcols;
+  int zchunks;      // z chunks per block of the z solves (8 or 16; 0: chosen by the launcher)
 };
+
+// side streams and events of the banded 3D x-y pass: the inverse y
+// transforms of every band run on y1, the x passes on the stage's stream, the
+// forward y transforms on y2, each band waiting only for what it reads
+constexpr int kMaxBands = 8;
+struct XYAux {
+  cudaStream_t y1, y2;
+  cudaEvent_t fork, join;
+  cudaEvent_t ev_ify[kMaxBands], ev_x[kMaxBands];
+  int bands;
+};
+
+// one block's work in an ensemble launch: member solver `run`, block
+// coordinate x (x-pass level column or z-solve mode group), and for the x
+// pass the slab height S and slabs per block
+struct EnsItem {
+  int run, x, S, iters;
+};
+constexpr int kEnsThreads = 256;
 
 // launchers (sf_kernels.cu); each returns the number of kernels launched
 int prepare_kernels();
 // one stage; if ev != nullptr, ev[i] is recorded after the i-th kernel
-int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev = nullptr);
+int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev = nullptr, const XYAux* aux = nullptr);
 int stage_kernel_count(const Geo& g);
 const char* stage_kernel_name(const Geo& g, int i);
 int launch_project(const StageArgs& a, cudaStream_t st);  // RemoveDivergence only
@@ -101,6 +125,14 @@ int launch_gather_ref(const Geo& g, const float2* ref, float2* kept, cudaStream_
 int launch_scatter_ref(const Geo& g, const float2* kept, float2* ref, cudaStream_t st);
 int launch_energy(const Geo& g, const float2* Sa, const float2* Sb, int nrun_pairs,
                   const float* zc, const float* Ri, double* out, cudaStream_t st);
+// ensembles of 2D solvers of different grids (sf_ensemble): every member's
+// x pass in one launch and every member's z step in another; args holds one
+// StageArgs per member
+size_t ensemble_xpass_smem(int N1, int S);
+size_t ensemble_zstep_smem(int N3);
+int launch_xpass_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st);
+int launch_zstep_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st);
+int prepare_ensemble_kernels();
 int launch_grad_sq(const Geo& g, const float2* S, int nruns, const float* zc, const double* kxd, const double* kyd,
                    double* out, cudaStream_t st);
 int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* base_out,

@@ -7,9 +7,11 @@
 //                   1/(N1 N2), 2/3 truncation and the z stencils and
 //                   x-derivatives that follow each product
 //   [3D] k_fft_y    (kx, y) -> (kx, ky), y-derivatives, sum into r
-//        k_z_cn_chunked    per (mode, field): ExplicitRK + linear buoyancy terms +
-//                          FinishRHS + CrankNicolson right-hand side + Thomas solve
-//        k_z_proj_chunked  per mode: divergence, Laplacian solve, projection, p update
+//        k_z_step   per group of 16 modes: for every field ExplicitRK + linear
+//                   buoyancy terms + FinishRHS + CrankNicolson right-hand side +
+//                   Thomas solve, then the divergence, Laplacian solve,
+//                   projection and p update (k_z_proj_chunked alone serves
+//                   RemoveDivergence outside a step)
 // Every kernel touches only kept (dealiased) modes, which is all the reference's
 // ModalField arithmetic touches (Field.h:1129-1166).
 
@@ -40,7 +42,7 @@ __global__ void __launch_bounds__(kYThreads, 8) k_ifft_y(StageArgs a) {
   __shared__ float2 fbuf[(kYThreads / G) * BUF];
   const int lane = threadIdx.x & 31, grp = threadIdx.x / G, l = threadIdx.x % G;
   const int j1 = blockIdx.x * ycols<N2>() + grp;
-  const int j = blockIdx.y;
+  const int j = blockIdx.y + a.lvl0;
   const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
   const bool act = j1 < g.K1;
   const float2* src = a.S + ((size_t)(run * 5 + f) * g.N3 + j) * g.Pp;
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
   __shared__ float2 fbuf[(kYThreads / G) * BUF];
   const int grp = threadIdx.x / G, l = threadIdx.x % G;
   const int j1 = blockIdx.x * ycols<N2>() + grp;
-  const int j = blockIdx.y;
+  const int j = blockIdx.y + a.lvl0;
   const int run = blockIdx.z >> 2, f = blockIdx.z & 3;
   const bool act = j1 < g.K1;
   const float2* cA = a.mixout + ((size_t)(run * 8 + 2 * f) * g.N3 + j) * N2 * g.K1 + j1;
@@ -141,6 +143,11 @@ __host__ __device__ __forceinline__ bool carried(int p) {
   return p == P_Q1 || p == P_QB || p == P_Q2 || p == P_P4;
 }
 
+// row stride (floats) of the nodal rows in shared memory: N1 padded by one
+// lane group, so the lane groups of a warp, which read the same field at
+// consecutive slots, fall on different banks
+__host__ __device__ constexpr int nod_row(int N1) { return N1 + (N1 >= 256 ? 16 : (N1 >= 64 ? 8 : 4)); }
+
 struct XLayout {  // shared-memory carve-up of k_xpass
   int nprod, nrows;
   size_t hat_off, stage_off, buf_off, nod_off, base_off, carry_off, bytes;
@@ -167,8 +174,8 @@ __host__ __device__ inline XLayout x_layout(int S, int N1, int K1, int dim3, int
     L.stage_off = off; off += (hat > stage ? hat : stage);
   }
   L.buf_off = off;  off += sizeof(float2) * (size_t)ngroups * bufstride;
-  L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * N1;
-  L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * N1;
+  L.nod_off = off;  off += sizeof(float) * (size_t)4 * (S + 2) * nod_row(N1);
+  L.base_off = off; if (linear) off += sizeof(float) * (size_t)4 * (S + 2) * nod_row(N1);
   L.carry_off = off; off += sizeof(float2) * (size_t)4 * K1;   // transformed rows kept for the next slab
   L.bytes = off;
   return L;
@@ -213,7 +220,7 @@ __device__ __forceinline__ HalfC half_coeffs(int s, int j0, int N3, const float*
 // leaves out its x-independent U_^2 part, which ddx multiplies by zero)
 template <int P, int N1>
 __device__ __forceinline__ float prod_at(const float* nod, int NS, const HalfC& c, int n) {
-  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * N1 + n]; };
+  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * nod_row(N1) + n]; };
   float v;
   if constexpr (P == P_S1) { const float a = u(0, c.s); v = a * (a + 2.f * c.ub); }
   else if constexpr (P == P_SB1) v = (u(0, c.s) + c.ub) * u(3, c.s);
@@ -236,8 +243,8 @@ __device__ __forceinline__ float prod_at(const float* nod, int NS, const HalfC& 
 // U1b + U_, U2b, U3b, Bb (so the U_ terms come with the base's u1)
 template <int P, int N1>
 __device__ __forceinline__ float prod_at_lin(const float* nod, const float* bas, int NS, const HalfC& c, int n) {
-  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * N1 + n]; };
-  auto U = [&](int f, int slot) { return bas[(f * NS + slot) * N1 + n]; };
+  auto u = [&](int f, int slot) { return nod[(f * NS + slot) * nod_row(N1) + n]; };
+  auto U = [&](int f, int slot) { return bas[(f * NS + slot) * nod_row(N1) + n]; };
   float v;
   if constexpr (P == P_S1) v = (2.f * u(0, c.s)) * U(0, c.s);
   else if constexpr (P == P_SB1) v = u(3, c.s) * U(0, c.s) + U(3, c.s) * u(0, c.s);
@@ -295,8 +302,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // two top nodal levels and the top transformed rows of the carried products
 // (their z stencils reach one level across the slab boundary), so each level
 // is transformed once rather than once per slab that touches it.
+// The body of one x-pass block: (bx, by, bz) = (level column, y row, run)
+// relative to a.xcol0 and a.run_offset, so that a kernel over many solvers'
+// work items can run it for any block of any of them.
 template <int N1, bool LINEAR>
-__global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int iters) {
+__device__ __forceinline__ void xpass_body(const StageArgs& a, int S, int iters, int bx, int by, int bz) {
   constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, BUF = fft_buf_stride<N1>();
   const int NGB = blockDim.x / G;   // lane groups per block
   const Geo g = a.g;
@@ -305,12 +315,13 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   const XLayout L = x_layout(S, N1, g.K1, g.dim3, LINEAR, BUF, NGB, tlm, iters > 1);
   float2* hat = reinterpret_cast<float2*>(xsm + L.hat_off);
   float2* stg = reinterpret_cast<float2*>(xsm + L.stage_off);  // phase A input rows [4 or 8][S+2][K1]
-  float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][N1]: U1, U2, U3, B
-  float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][N1]: U1b+Ubar, U2b, U3b, Bb
+  constexpr int NR = nod_row(N1);   // nodal row stride
+  float* nod = reinterpret_cast<float*>(xsm + L.nod_off);      // [4][S+2][NR]: U1, U2, U3, B
+  float* bnod = reinterpret_cast<float*>(xsm + L.base_off);    // [4][S+2][NR]: U1b+Ubar, U2b, U3b, Bb
   constexpr int K1 = N1 / 3;   // kept x modes (the solver's K1), a compile-time constant here
   const int N3 = g.N3;
-  const int y = blockIdx.y;
-  const int run = blockIdx.z + a.run_offset;
+  const int y = by;
+  const int run = bz + a.run_offset;
   const int brun = tlm ? (run - tlm) % tlm : run;   // run that holds the base state
   const int gid = threadIdx.x / G, l = threadIdx.x % G;
   float2* buf = reinterpret_cast<float2*>(xsm + L.buf_off) + (size_t)gid * BUF;
@@ -351,10 +362,11 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
       }
     }
   };
-  stage_rows(blockIdx.x * iters * S, 0);
+  const int col = bx + a.xcol0;   // level column of this block
+  stage_rows(col * iters * S, 0);
 
   for (int it = 0; it < iters; it++) {
-  const int j0 = (blockIdx.x * iters + it) * S;
+  const int j0 = (col * iters + it) * S;
   if (j0 >= N3) break;
   const int s0 = it == 0 ? 0 : 2;   // nodal slots 0, 1 come from the slab below
   const int NSn = NS - s0;
@@ -363,7 +375,7 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
     const int nw = blockDim.x >> 5, lane = threadIdx.x & 31;
     for (int row = threadIdx.x >> 5; row < 4 * NS; row += nw) {
       const int f = row / NS, t = j0 - 1 + row - f * NS;
-      float* d = bnod + (size_t)row * N1;
+      float* d = bnod + (size_t)row * NR;
       if (t < 0 || t >= N3 || (f == 1 && !g.dim3)) {
         for (int x = lane; x < N1; x += 32) d[x] = 0.f;
       } else {
@@ -376,8 +388,8 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
   __syncthreads();
   if (LINEAR && !tlm) {   // U1b + U_ as nnTemp (phase A writes only the own rows meanwhile)
     for (int i = threadIdx.x; i < NS * N1; i += blockDim.x) {
-      const int t = j0 - 1 + i / N1;
-      if (t >= 0 && t < N3) bnod[i] += Ub[t];
+      const int sl = i / N1, t = j0 - 1 + sl;
+      if (t >= 0 && t < N3) bnod[sl * NR + (i - sl * N1)] += Ub[t];
     }
   }
 
@@ -412,8 +424,8 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
     fft_inv(x);
     if (valid) {
       float* rows = ofs ? bnod : nod;
-      float* rA = rows + ((size_t)fA * NS + s) * N1;
-      float* rB = rows + ((size_t)fB * NS + s) * N1;
+      float* rA = rows + ((size_t)fA * NS + s) * NR;
+      float* rB = rows + ((size_t)fB * NS + s) * NR;
       const int t = j0 - 1 + s;
       // the base's U1 row carries U_ (nnTemp = U1_tot + U_, IMEXRK.cpp:212)
       const float add = (ofs && fA == 0 && t >= 0 && t < N3) ? a.Ubar[(size_t)brun * N3 + t] : 0.f;
@@ -555,11 +567,16 @@ __global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int 
       const int fb = i / (2 * N1), r = i - fb * 2 * N1, sl = r / N1, x = r - sl * N1;
       float* rows = fb < 4 ? nod : bnod;
       const int f = fb & 3;
-      rows[((size_t)f * NS + sl) * N1 + x] = rows[((size_t)f * NS + S + sl) * N1 + x];
+      rows[((size_t)f * NS + sl) * NR + x] = rows[((size_t)f * NS + S + sl) * NR + x];
     }
     __syncthreads();
   }
   }   // slabs
+}
+
+template <int N1, bool LINEAR>
+__global__ void __launch_bounds__(kXMaxThreads) k_xpass(StageArgs a, int S, int iters) {
+  xpass_body<N1, LINEAR>(a, S, iters, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ============================================================ z pass ====
@@ -622,19 +639,19 @@ __device__ __forceinline__ void load_iden(float (&bi)[K], const float* __restric
   }
 }
 
-// the body of k_z_cn_chunked for field f of family FAM (0: u1 and u2,
+// the CN solve of k_z_step for field f of family FAM (0: u1 and u2,
 // 1: u3, Dirichlet; 2: b), so that each family's loads and terms are fixed
 // at compile time; IC: chunks clear of the ends take sweeps without the
 // per-level end tests
 template <int ZW, int FAM, bool IC>
-__device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
+__device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f, const int bx, const int bz) {
   const Geo g = a.g;
   extern __shared__ float zsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int m0 = blockIdx.x * 16 + (lane >> 1), c = lane & 1;
+  const int m0 = bx * 16 + (lane >> 1), c = lane & 1;
   const bool act = m0 < g.P;
   const int m = act ? m0 : 0;
-  const int run = blockIdx.z;
+  const int run = bz;
   const int N3 = g.N3, Pp = g.Pp;
   const int chunk = (N3 + ZW - 1) / ZW;
   const int js = min(N3, w * chunk), je = min(N3, js + chunk);
@@ -798,35 +815,21 @@ __device__ __forceinline__ void z_cn_body(const StageArgs& a, const int f) {
   else sweep3(std::false_type{});
 }
 
-// k_z_cn with the chunked solve: ExplicitRK, linear buoyancy terms,
-// FinishRHS, CrankNicolson and the Thomas solve of one field for 16 modes
-template <int ZW, bool IC>
-__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_cn_chunked(StageArgs a) {
-  const int fi = blockIdx.y;
-  const int f = a.g.dim3 ? fi : (fi == 0 ? 0 : fi + 1);   // 2D: u1, u3, b
-  if (f <= 1)
-    z_cn_body<ZW, 0, IC>(a, f);
-  else if (f == 2)
-    z_cn_body<ZW, 1, IC>(a, f);
-  else
-    z_cn_body<ZW, 2, IC>(a, f);
-}
-
 // RemoveDivergence with the chunked solve, for 16 modes per block: the
 // divergence and the Laplacian factors upward, q downward, then u -= grad q
 // and p += pm q. The two components of a mode are adjacent lanes and
 // exchange q; u3_{j+1} at a chunk's top uses the next chunk's q from the scan.
 template <int ZW>
-__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
-                                                           const float* zc, const float* fa, const float* fc,
-                                                           const float* inv_den, const float* kx, const float* ky,
-                                                           float pm) {
+__device__ __forceinline__ void z_proj_body(const Geo& g, float2* U, const float2* Psrc, float2* Pdst,
+                                            const float* zc, const float* fa, const float* fc,
+                                            const float* inv_den, const float* kx, const float* ky, float pm,
+                                            const int bx, const int bz) {
   extern __shared__ float zsm[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int m0 = blockIdx.x * 16 + (lane >> 1), c = lane & 1;
+  const int m0 = bx * 16 + (lane >> 1), c = lane & 1;
   const bool act = m0 < g.P;
   const int m = act ? m0 : 0;
-  const int run = blockIdx.z;
+  const int run = bz;
   const int N3 = g.N3, Pp = g.Pp;
   const int chunk = (N3 + ZW - 1) / ZW;
   const int js = min(N3, w * chunk), je = min(N3, js + chunk);
@@ -942,6 +945,75 @@ __global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo
       qn = qj;
     }
   }
+}
+
+template <int ZW>
+__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_proj_chunked(Geo g, float2* U, const float2* Psrc, float2* Pdst,
+                                                           const float* zc, const float* fa, const float* fc,
+                                                           const float* inv_den, const float* kx, const float* ky,
+                                                           float pm) {
+  z_proj_body<ZW>(g, U, Psrc, Pdst, zc, fa, fc, inv_den, kx, ky, pm, blockIdx.x, blockIdx.z);
+}
+
+// The whole z pass of a stage for 16 modes per block: the CN solves of every
+// field (ExplicitRK, linear buoyancy terms, FinishRHS, CrankNicolson and the
+// Thomas solve, IMEXRK.cpp:75-134), then RemoveDivergence on the new
+// velocities (IMEXRK.cpp:43-73). The projection reads the velocities this
+// block has just written (visible to the block after the barrier, and still
+// in L2), so the pass makes one trip through HBM instead of two kernels'.
+// Every field's solve uses the same shared-memory rows: a thread reads and
+// writes only its own rows of sD, and the chunk scans synchronise the block.
+template <int ZW, bool IC>
+__device__ __forceinline__ void z_step_body(const StageArgs& a, const int bx, const int bz) {
+  if (a.g.dim3) {
+    z_cn_body<ZW, 0, IC>(a, 0, bx, bz);
+    z_cn_body<ZW, 0, IC>(a, 1, bx, bz);
+  } else {
+    z_cn_body<ZW, 0, IC>(a, 0, bx, bz);
+  }
+  z_cn_body<ZW, 1, IC>(a, 2, bx, bz);
+  z_cn_body<ZW, 2, IC>(a, 3, bx, bz);
+  __syncthreads();
+  z_proj_body<ZW>(a.g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc, a.inv_den, a.kx, a.ky, a.pm, bx, bz);
+}
+
+template <int ZW, bool IC>
+__global__ void __launch_bounds__(ZW * 32, ZW == 8 ? 3 : 1) k_z_step(StageArgs a) {
+  z_step_body<ZW, IC>(a, blockIdx.x, blockIdx.z);
+}
+
+
+// ============================================================ ensembles ====
+// Every member of an ensemble of 2D solvers (grids of different sizes, one
+// run each) in one launch per kernel: a block reads its work item and its
+// member's stage arguments and runs the same block body as the solver's own
+// launch would. Blocks have kEnsThreads threads for every grid; the dynamic
+// shared memory is the largest any member needs.
+__global__ void __launch_bounds__(kEnsThreads, 2) k_xpass_ens(const StageArgs* __restrict__ args,
+                                                              const EnsItem* __restrict__ items) {
+  __shared__ StageArgs sa;
+  const EnsItem it = items[blockIdx.x];
+  if (threadIdx.x == 0) sa = args[it.run];
+  __syncthreads();
+  switch (sa.g.N1) {
+    case 16: xpass_body<16, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    case 32: xpass_body<32, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    case 64: xpass_body<64, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    case 128: xpass_body<128, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    case 256: xpass_body<256, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    case 512: xpass_body<512, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+    default: break;
+  }
+}
+
+__global__ void __launch_bounds__(kEnsThreads, 2) k_zstep_ens(const StageArgs* __restrict__ args,
+                                                              const EnsItem* __restrict__ items) {
+  __shared__ StageArgs sa;
+  const EnsItem it = items[blockIdx.x];
+  if (threadIdx.x == 0) sa = args[it.run];
+  __syncthreads();
+  if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
+  else z_step_body<8, false>(sa, it.x, 0);
 }
 
 
@@ -1118,8 +1190,14 @@ __global__ void k_grad_sq(Geo g, const float2* __restrict__ S, const float* __re
 // ======================================================== launchers ====
 static inline unsigned cdiv(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
 
+struct XShape {
+  int S, iters, threads;
+  size_t bytes;
+};
+
+// launch shape of the x pass: slab height S, slabs per block, threads, bytes
 template <int N1, bool LIN>
-static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
+static XShape xpass_shape(const StageArgs& a, int nruns) {
   const Geo& g = a.g;
   const int tlm = LIN ? a.tlm : 0;
   constexpr int G = FFTShape<N1>::G, BUF = fft_buf_stride<N1>();
@@ -1155,8 +1233,36 @@ static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
     iters++;
   if (a.xslabs > 0) iters = std::min<int>(a.xslabs, (int)cdiv(g.N3, S));
   if (iters > 1 && bytes(S, 1) > 227 * 1024) iters = 1;   // no room for the prefetch buffer
-  dim3 grid(cdiv(g.N3, S * iters), g.N2, nruns);
-  k_xpass<N1, LIN><<<grid, threads(S), bytes(S, iters > 1), st>>>(a, S, iters);
+  return XShape{S, iters, threads(S), bytes(S, iters > 1)};
+}
+
+// one launch over the level columns a.xcol0 .. a.xcol0 + a.xcols - 1 (all
+// when a.xcols = 0); a column is the S * iters levels one block walks through
+template <int N1, bool LIN>
+static void xpass_launch(const StageArgs& a, int nruns, cudaStream_t st) {
+  const Geo& g = a.g;
+  const XShape x = xpass_shape<N1, LIN>(a, nruns);
+  const int ncol = (int)cdiv(g.N3, x.S * x.iters);
+  const int cols = a.xcols > 0 ? a.xcols : ncol - a.xcol0;
+  dim3 grid(cols, g.N2, nruns);
+  k_xpass<N1, LIN><<<grid, x.threads, x.bytes, st>>>(a, x.S, x.iters);
+}
+
+template <int N1>
+static int xpass_col_levels(const StageArgs& a, bool L, int nruns) {
+  const XShape x = L ? xpass_shape<N1, true>(a, nruns) : xpass_shape<N1, false>(a, nruns);
+  return x.S * x.iters;
+}
+
+static int xpass_column_levels(const StageArgs& a, bool L, int nruns) {
+  switch (a.g.N1) {
+    case 16: return xpass_col_levels<16>(a, L, nruns);
+    case 32: return xpass_col_levels<32>(a, L, nruns);
+    case 64: return xpass_col_levels<64>(a, L, nruns);
+    case 128: return xpass_col_levels<128>(a, L, nruns);
+    case 256: return xpass_col_levels<256>(a, L, nruns);
+    default: return xpass_col_levels<512>(a, L, nruns);
+  }
 }
 
 static void launch_xpass_runs(const StageArgs& a, bool L, int nruns, cudaStream_t st) {
@@ -1191,11 +1297,13 @@ static int launch_xpass(const StageArgs& a, cudaStream_t st) {
 // field of a single run (nz = 1) reads and writes that field only
 template <int N2>
 static void ify_launch(const StageArgs& a, int nz, cudaStream_t st) {
-  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, nz), kYThreads, 0, st>>>(a);
+  const int nl = a.nlvl > 0 ? a.nlvl : a.g.N3 - a.lvl0;
+  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), nl, nz), kYThreads, 0, st>>>(a);
 }
 template <int N2>
 static void fy_launch(const StageArgs& a, cudaStream_t st) {
-  k_fft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), a.g.N3, a.g.nrun * 4), kYThreads, 0, st>>>(a);
+  const int nl = a.nlvl > 0 ? a.nlvl : a.g.N3 - a.lvl0;
+  k_fft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), nl, a.g.nrun * 4), kYThreads, 0, st>>>(a);
 }
 static void launch_ifft_y_z(const StageArgs& a, int nz, cudaStream_t st) {
   switch (a.g.N2) {
@@ -1231,8 +1339,8 @@ int prepare_kernels() {
   ATTR((k_xpass<128, false>)) ATTR((k_xpass<256, false>)) ATTR((k_xpass<512, false>))
   ATTR((k_xpass<16, true>)) ATTR((k_xpass<32, true>)) ATTR((k_xpass<64, true>))
   ATTR((k_xpass<128, true>)) ATTR((k_xpass<256, true>)) ATTR((k_xpass<512, true>))
-  ATTR((k_z_cn_chunked<8, false>)) ATTR((k_z_cn_chunked<8, true>)) ATTR((k_z_cn_chunked<16, false>))
-  ATTR((k_z_cn_chunked<16, true>)) ATTR(k_z_proj_chunked<8>) ATTR(k_z_proj_chunked<16>)
+  ATTR(k_z_proj_chunked<8>) ATTR(k_z_proj_chunked<16>)
+  ATTR((k_z_step<8, false>)) ATTR((k_z_step<8, true>)) ATTR((k_z_step<16, false>)) ATTR((k_z_step<16, true>))
 #undef ATTR
   return e == cudaSuccess ? 0 : -1;
 }
@@ -1245,28 +1353,10 @@ static int z_chunks(const Geo& g, int fields) {
   return (long long)cdiv(g.P, 16) * fields * g.nrun < 148 ? 16 : 8;
 }
 
-// the CN solves of a stage; chunks of 48 levels or more take the variant
-// with end-test-free interior sweeps (measured 7% faster at 384 levels in 8
-// chunks, and slower with 32-level chunks, where it is not used)
-static void launch_z_cn(const StageArgs& a, cudaStream_t st) {
-  const Geo& g = a.g;
-  const int nf = g.dim3 ? 4 : 3;
-  const dim3 zgrid(cdiv(g.P, 16), nf, g.nrun);
-  const int zw = z_chunks(g, nf);
-  const bool ic = cdiv(g.N3, zw) >= 48;
-  if (zw == 16) {
-    if (ic) k_z_cn_chunked<16, true><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
-    else k_z_cn_chunked<16, false><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
-  } else {
-    if (ic) k_z_cn_chunked<8, true><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
-    else k_z_cn_chunked<8, false><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
-  }
-}
-
 int launch_project(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
   const dim3 grid(cdiv(g.P, 16), 1, g.nrun);
-  if (z_chunks(g, 1) == 16)
+  if ((a.zchunks ? a.zchunks : z_chunks(g, 1)) == 16)
     k_z_proj_chunked<16><<<grid, 16 * 32, zchunk_smem(g, 16), st>>>(g, a.Sn, a.S, a.Sn, a.zc, a.fa, a.fc,
                                                                       a.inv_den, a.kx, a.ky, a.pm);
   else
@@ -1275,15 +1365,82 @@ int launch_project(const StageArgs& a, cudaStream_t st) {
   return 1;
 }
 
+// the merged z pass (CN solves of every field, then the projection): one
+// block per 16 modes, so the chunk count follows from the mode groups alone;
+// chunks of 48 levels or more take the variant with end-test-free interior
+// sweeps (measured 7% faster at 384 levels in 8 chunks, and slower with
+// 32-level chunks, where it is not used)
+static void launch_z_step(const StageArgs& a, cudaStream_t st) {
+  const Geo& g = a.g;
+  const dim3 zgrid(cdiv(g.P, 16), 1, g.nrun);
+  const int zw = a.zchunks ? a.zchunks : z_chunks(g, 1);
+  const bool ic = cdiv(g.N3, zw) >= 48;
+  if (zw == 16) {
+    if (ic) k_z_step<16, true><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+    else k_z_step<16, false><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);
+  } else {
+    if (ic) k_z_step<8, true><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+    else k_z_step<8, false><<<zgrid, 8 * 32, zchunk_smem(g, 8), st>>>(a);
+  }
+}
+
 const char* stage_kernel_name(const Geo& g, int i) {
-  static const char* n3[] = {"k_ifft_y", "k_xpass", "k_fft_y", "k_z_cn", "k_z_proj"};
-  static const char* n2[] = {"k_xpass", "k_z_cn", "k_z_proj"};
+  static const char* n3[] = {"k_ifft_y", "k_xpass", "k_fft_y", "k_z_step"};
+  static const char* n2[] = {"k_xpass", "k_z_step"};
   return g.dim3 ? n3[i] : n2[i];
 }
-int stage_kernel_count(const Geo& g) { return g.dim3 ? 5 : 3; }
+int stage_kernel_count(const Geo& g) { return g.dim3 ? 4 : 2; }
 
-int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
+// The 3D x-y pass in level bands: band b's inverse y transforms (stream y1,
+// all bands back to back), x pass (the stage's stream, after the inverse
+// transforms of its own band and of the band above, whose lowest level its
+// z stencils read) and forward y transforms (stream y2, after that band's x
+// pass). The memory-bound y transforms of the other bands then run beside the
+// compute-bound x pass instead of before and after it. Bands follow the x
+// pass's block columns, so no block straddles two bands.
+static int launch_xy_banded(const StageArgs& a, cudaStream_t st, const XYAux& aux) {
   const Geo& g = a.g;
+  const int lv = xpass_column_levels(a, a.linear != 0, g.nrun);
+  const int ncol = (int)cdiv(g.N3, lv);
+  const int B = std::min(std::min(aux.bands, kMaxBands), ncol);
+  auto c0 = [&](int b) { return (int)((long long)ncol * b / B); };
+  auto band = [&](int b) {
+    StageArgs y = a;
+    y.lvl0 = c0(b) * lv;
+    y.nlvl = std::min(g.N3, c0(b + 1) * lv) - y.lvl0;
+    return y;
+  };
+  cudaEventRecord(aux.fork, st);
+  cudaStreamWaitEvent(aux.y1, aux.fork, 0);
+  cudaStreamWaitEvent(aux.y2, aux.fork, 0);
+  for (int b = 0; b < B; b++) {
+    launch_ifft_y(band(b), g.nrun, aux.y1);
+    cudaEventRecord(aux.ev_ify[b], aux.y1);
+  }
+  for (int b = 0; b < B; b++) {
+    cudaStreamWaitEvent(st, aux.ev_ify[std::min(b + 1, B - 1)], 0);
+    StageArgs x = a;
+    x.xcol0 = c0(b);
+    x.xcols = c0(b + 1) - c0(b);
+    launch_xpass(x, st);
+    cudaEventRecord(aux.ev_x[b], st);
+  }
+  for (int b = 0; b < B; b++) {
+    cudaStreamWaitEvent(aux.y2, aux.ev_x[b], 0);
+    launch_fft_y(band(b), aux.y2);
+  }
+  cudaEventRecord(aux.join, aux.y2);
+  cudaStreamWaitEvent(st, aux.join, 0);
+  return 3 * B;
+}
+
+int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev, const XYAux* aux) {
+  const Geo& g = a.g;
+  if (g.dim3 && aux && aux->bands > 1 && !ev && !a.tlm) {
+    const int n = launch_xy_banded(a, st, *aux);
+    launch_z_step(a, st);
+    return n + 1;
+  }
   int n = 0;
   auto mark = [&]() {
     if (ev) cudaEventRecord(ev[n], st);
@@ -1299,17 +1456,14 @@ int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev) {
     launch_fft_y(a, st);
     mark();
   }
-  launch_z_cn(a, st);
-  mark();
-  launch_project(a, st);
+  launch_z_step(a, st);
   mark();
   return n + extra;
 }
 
 int launch_z_solves(const StageArgs& a, cudaStream_t st) {
-  launch_z_cn(a, st);
-  launch_project(a, st);
-  return 2;
+  launch_z_step(a, st);
+  return 1;
 }
 
 int launch_factor(const Geo& g, const double* bands, const double* kx, const double* ky, double h0, double h1,
@@ -1326,6 +1480,38 @@ int launch_gather_ref(const Geo& g, const float2* ref, float2* kept, cudaStream_
 int launch_scatter_ref(const Geo& g, const float2* kept, float2* ref, cudaStream_t st) {
   k_scatter_ref<<<dim3(cdiv(g.P, 32), cdiv(g.N3, 32)), dim3(32, 8), 0, st>>>(g, kept, ref);
   return 1;
+}
+
+static int fft_G(int N) { return N >= 256 ? 16 : (N >= 64 ? 8 : 4); }
+static int fft_bufstride(int N) {
+  switch (N) {
+    case 16: return fft_buf_stride<16>();
+    case 32: return fft_buf_stride<32>();
+    case 64: return fft_buf_stride<64>();
+    case 128: return fft_buf_stride<128>();
+    case 256: return fft_buf_stride<256>();
+    default: return fft_buf_stride<512>();
+  }
+}
+
+size_t ensemble_xpass_smem(int N1, int S) {
+  return x_layout(S, N1, N1 / 3, 0, 0, fft_bufstride(N1), kEnsThreads / fft_G(N1), 0, 0).bytes;
+}
+size_t ensemble_zstep_smem(int N3) { return sizeof(float) * ((size_t)N3 * 32 + 3 * 8 * 32); }
+
+int launch_xpass_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st) {
+  k_xpass_ens<<<nitems, kEnsThreads, smem, st>>>(args, items);
+  return 1;
+}
+int launch_zstep_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st) {
+  k_zstep_ens<<<nitems, kEnsThreads, smem, st>>>(args, items);
+  return 1;
+}
+int prepare_ensemble_kernels() {
+  const int lim = 227 * 1024 - (int)sizeof(StageArgs) - 64;
+  cudaError_t e = cudaFuncSetAttribute(k_xpass_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zstep_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  return e == cudaSuccess ? 0 : -1;
 }
 
 int launch_grad_sq(const Geo& g, const float2* S, int nruns, const float* zc, const double* kxd, const double* kyd,

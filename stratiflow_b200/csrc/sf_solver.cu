@@ -2,6 +2,7 @@
 // step sequencer (one CUDA graph per step, replayed).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -53,6 +54,9 @@ struct sf_solver {
   bool base_set = false;
   int tlm = 0;                   // tangent-linear batch (sf_set_tangent)
   int xslabs = 0;                // slabs per x-pass block (sf_set_xpass_slabs)
+  XYAux xy{};                    // side streams of the banded 3D x-y pass
+  int xy_bands = 1;              // level bands of the 3D x-y pass (sf_set_xy_bands)
+  int zchunks = 0;               // z chunks per z-solve block (sf_set_z_chunks)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -111,6 +115,17 @@ static void free_all(sf_solver* s) {
     if (P->d2h) cudaStreamDestroy(P->d2h);
     delete P;
     s->pipe = nullptr;
+  }
+  if (s->xy.y1) cudaStreamDestroy(s->xy.y1);
+  if (s->xy.y2) cudaStreamDestroy(s->xy.y2);
+  {
+    cudaEvent_t* evs[] = {&s->xy.fork, &s->xy.join};
+    for (cudaEvent_t* e : evs)
+      if (*e) cudaEventDestroy(*e);
+    for (int b = 0; b < kMaxBands; b++) {
+      if (s->xy.ev_ify[b]) cudaEventDestroy(s->xy.ev_ify[b]);
+      if (s->xy.ev_x[b]) cudaEventDestroy(s->xy.ev_x[b]);
+    }
   }
   if (s->st) cudaStreamDestroy(s->st);
 }
@@ -203,6 +218,7 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.tlm = linear ? 0 : s->tlm;
   a.run_offset = 0;
   a.xslabs = s->xslabs;
+  a.zchunks = s->zchunks;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -219,7 +235,8 @@ static int record_step(sf_solver* s, int par, bool linear) {
   int cur = par;
   for (int k = 0; k < 3; k++) {
     StageArgs a = stage_args(s, k, cur, linear);
-    n += launch_stage(a, s->st);
+    s->xy.bands = s->xy_bands;
+    n += launch_stage(a, s->st, nullptr, s->g.dim3 && s->xy.y1 ? &s->xy : nullptr);
     cur = 1 - cur;
   }
   return n;
@@ -296,6 +313,16 @@ int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, s
   if (prepare_kernels() != 0 || prepare_adjoint_kernels() != 0)
     return cleanup_fail(fail(SF_ECUDA, "cudaFuncSetAttribute failed"));
   CKC(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking));
+  if (g.dim3) {
+    CKC(cudaStreamCreateWithFlags(&s->xy.y1, cudaStreamNonBlocking));
+    CKC(cudaStreamCreateWithFlags(&s->xy.y2, cudaStreamNonBlocking));
+    CKC(cudaEventCreateWithFlags(&s->xy.fork, cudaEventDisableTiming));
+    CKC(cudaEventCreateWithFlags(&s->xy.join, cudaEventDisableTiming));
+    for (int b = 0; b < kMaxBands; b++) {
+      CKC(cudaEventCreateWithFlags(&s->xy.ev_ify[b], cudaEventDisableTiming));
+      CKC(cudaEventCreateWithFlags(&s->xy.ev_x[b], cudaEventDisableTiming));
+    }
+  }
   const size_t cb = sizeof(float2);
   CKC(cudaMalloc(&s->S[0], cb * nrun * 5 * g.fblk));
   CKC(cudaMalloc(&s->S[1], cb * nrun * 5 * g.fblk));
@@ -789,6 +816,25 @@ int sf_cfl(sf_solver* s, int run, double* cfl) {
   return SF_OK;
 }
 
+int sf_set_z_chunks(sf_solver* s, int chunks) {
+  if (!s || !(chunks == 0 || chunks == 8 || chunks == 16)) return fail(SF_EINVAL, "chunks must be 0, 8 or 16");
+  if (s->g.N3 < 2 * (chunks ? chunks : 8)) return fail(SF_EINVAL, "too few levels for that many chunks");
+  if (chunks != s->zchunks) {
+    s->zchunks = chunks;
+    drop_graphs(s);
+  }
+  return SF_OK;
+}
+
+int sf_set_xy_bands(sf_solver* s, int bands) {
+  if (!s || bands < 1 || bands > kMaxBands) return fail(SF_EINVAL, "bands must be in [1, 8]");
+  if (bands != s->xy_bands) {
+    s->xy_bands = bands;
+    drop_graphs(s);
+  }
+  return SF_OK;
+}
+
 int sf_set_xpass_slabs(sf_solver* s, int slabs) {
   if (!s || slabs < 0) return fail(SF_EINVAL, "bad argument");
   if (slabs != s->xslabs) {
@@ -828,6 +874,210 @@ int sf_stream(sf_solver* s, void** stream) {
 int sf_launch_count(sf_solver* s, long long* count) {
   if (!s || !count) return fail(SF_EINVAL, "bad argument");
   *count = s->launches;
+  return SF_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- ensembles
+// A batch of independent 2D runs on grids of different sizes: one member
+// solver per run (its own buffers, factors, Ri and background), stepped
+// together with one x-pass launch and one z-step launch per RK stage over the
+// work items of every member, captured as one CUDA graph per step parity.
+struct sf_ensemble {
+  int device = 0;
+  std::vector<sf_solver*> members;
+  cudaStream_t st = nullptr;
+  StageArgs* d_args = nullptr;   // [parity][stage][member]
+  std::vector<StageArgs> h_args;
+  EnsItem *d_x = nullptr, *d_z = nullptr;
+  int nx = 0, nz = 0;
+  size_t xsmem = 0, zsmem = 0;
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long launches = 0;
+};
+
+static void ens_free(sf_ensemble* e) {
+  for (cudaGraphExec_t& gx : e->graph)
+    if (gx) cudaGraphExecDestroy(gx);
+  if (e->d_args) cudaFree(e->d_args);
+  if (e->d_x) cudaFree(e->d_x);
+  if (e->d_z) cudaFree(e->d_z);
+  if (e->st) cudaStreamDestroy(e->st);
+  for (sf_solver* m : e->members)
+    if (m) sf_destroy(m);
+  delete e;
+}
+
+extern "C" {
+
+int sf_ensemble_create(int nrun, const sf_grid* grids, const sf_flow* flows, const double* dt, int device,
+                       sf_ensemble** out) {
+  if (nrun < 1 || !grids || !flows || !dt || !out) return fail(SF_EINVAL, "bad argument");
+  for (int r = 0; r < nrun; r++)
+    if (grids[r].N2 != 1) return fail(SF_EINVAL, "ensemble members are 2D grids (N2 = 1)");
+  CK(cudaSetDevice(device));
+  if (prepare_ensemble_kernels() != 0) return fail(SF_ECUDA, "cudaFuncSetAttribute failed (ensemble kernels)");
+  sf_ensemble* e = new sf_ensemble();
+  e->device = device;
+  for (int r = 0; r < nrun; r++) {
+    sf_grid g = grids[r];
+    g.nrun = 1;
+    sf_solver* m = nullptr;
+    const int rc = sf_create(&g, &flows[r], dt[r], device, &m);
+    if (rc != SF_OK) {
+      ens_free(e);
+      return rc;
+    }
+    e->members.push_back(m);
+  }
+  // work items, the largest members first; every x-pass block takes one
+  // 4-level slab (S = 4, no carried slabs)
+  std::vector<int> order(nrun);
+  for (int r = 0; r < nrun; r++) order[r] = r;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return (long long)grids[a].N1 * grids[a].N3 > (long long)grids[b].N1 * grids[b].N3;
+  });
+  std::vector<EnsItem> xi, zi;
+  for (int r : order) {
+    const Geo& g = e->members[r]->g;
+    const int S = 4;
+    for (int c = 0; c < (g.N3 + S - 1) / S; c++) xi.push_back(EnsItem{r, c, S, 1});
+    for (int q = 0; q < (g.P + 15) / 16; q++) zi.push_back(EnsItem{r, q, 0, 0});
+    e->xsmem = std::max(e->xsmem, ensemble_xpass_smem(g.N1, S));
+    e->zsmem = std::max(e->zsmem, ensemble_zstep_smem(g.N3));
+  }
+  e->nx = (int)xi.size();
+  e->nz = (int)zi.size();
+  cudaError_t ce = cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_x, sizeof(EnsItem) * xi.size());
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_z, sizeof(EnsItem) * zi.size());
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_args, sizeof(StageArgs) * 6 * nrun);
+  if (ce == cudaSuccess) ce = cudaMemcpy(e->d_x, xi.data(), sizeof(EnsItem) * xi.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemcpy(e->d_z, zi.data(), sizeof(EnsItem) * zi.size(), cudaMemcpyHostToDevice);
+  if (ce != cudaSuccess) {
+    ens_free(e);
+    return fail(ce == cudaErrorMemoryAllocation ? SF_ENOMEM : SF_ECUDA, std::string("ensemble: ") + cudaGetErrorString(ce));
+  }
+  e->h_args.resize((size_t)6 * nrun);
+  *out = e;
+  return SF_OK;
+}
+
+int sf_ensemble_destroy(sf_ensemble* e) {
+  if (!e) return fail(SF_EINVAL, "null ensemble");
+  cudaStreamSynchronize(e->st);
+  ens_free(e);
+  return SF_OK;
+}
+
+int sf_ensemble_member(sf_ensemble* e, int r, sf_solver** s) {
+  if (!e || !s || r < 0 || r >= (int)e->members.size()) return fail(SF_EINVAL, "bad argument");
+  *s = e->members[r];
+  return SF_OK;
+}
+
+int sf_ensemble_step(sf_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return fail(SF_EINVAL, "bad argument");
+  const int R = (int)e->members.size();
+  const int par = e->members[0]->cur;
+  for (sf_solver* m : e->members) {
+    if (m->cur != par) return fail(SF_ESTATE, "ensemble members are at different state parities");
+    if (m->tlm) return fail(SF_ESTATE, "ensemble members cannot be tangent-linear batches");
+    CK(cudaStreamSynchronize(m->st));   // the members' own work (set_state, prepare, ...) first
+  }
+  // the stage arguments of every member for both parities (h, factors and
+  // pointers may have changed since the last call); the graphs read them
+  // from the device table
+  for (int p = 0; p < 2; p++)
+    for (int k = 0; k < 3; k++) {
+      const int cur = (k == 1) ? 1 - p : p;
+      for (int r = 0; r < R; r++) {
+        StageArgs a = stage_args(e->members[r], k, cur, false);
+        a.xslabs = 1;
+        e->h_args[((size_t)p * 3 + k) * R + r] = a;
+      }
+    }
+  CK(cudaMemcpyAsync(e->d_args, e->h_args.data(), sizeof(StageArgs) * e->h_args.size(), cudaMemcpyHostToDevice,
+                     e->st));
+  for (int p = 0; p < 2; p++) {
+    if (e->graph[p]) continue;
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < 3; k++) {
+      const StageArgs* a = e->d_args + ((size_t)p * 3 + k) * R;
+      launch_xpass_ens(a, e->d_x, e->nx, e->xsmem, e->st);
+      launch_zstep_ens(a, e->d_z, e->nz, e->zsmem, e->st);
+    }
+    cudaError_t ce = cudaStreamEndCapture(e->st, &gr);
+    if (ce != cudaSuccess) return fail(SF_ECUDA, std::string("ensemble graph capture: ") + cudaGetErrorString(ce));
+    ce = cudaGraphInstantiate(&e->graph[p], gr, 0);
+    cudaGraphDestroy(gr);
+    if (ce != cudaSuccess) return fail(SF_ECUDA, std::string("ensemble graph: ") + cudaGetErrorString(ce));
+  }
+  int cur = par;
+  for (int i = 0; i < nsteps; i++) {
+    CK(cudaGraphLaunch(e->graph[cur], e->st));
+    e->launches += 6;
+    cur = 1 - cur;   // three stages flip the state buffer three times
+  }
+  for (sf_solver* m : e->members) m->cur = cur;
+  CK(cudaGetLastError());
+  return SF_OK;
+}
+
+int sf_ensemble_profile(sf_ensemble* e, int nsteps, double* ms_x, double* ms_z) {
+  if (!e || nsteps < 1 || !ms_x || !ms_z) return fail(SF_EINVAL, "bad argument");
+  // the graphs and the argument table, as a step sets them up
+  int rc = sf_ensemble_step(e, 0);
+  if (rc != SF_OK) return rc;
+  const int R = (int)e->members.size();
+  int cur = e->members[0]->cur;
+  cudaEvent_t ev[7];
+  for (cudaEvent_t& x : ev) CK(cudaEventCreate(&x));
+  double tx = 0, tz = 0;
+  for (int i = 0; i < nsteps; i++) {
+    CK(cudaEventRecord(ev[0], e->st));
+    for (int k = 0; k < 3; k++) {
+      const StageArgs* a = e->d_args + ((size_t)cur * 3 + k) * R;
+      launch_xpass_ens(a, e->d_x, e->nx, e->xsmem, e->st);
+      CK(cudaEventRecord(ev[1 + 2 * k], e->st));
+      launch_zstep_ens(a, e->d_z, e->nz, e->zsmem, e->st);
+      CK(cudaEventRecord(ev[2 + 2 * k], e->st));
+    }
+    CK(cudaEventSynchronize(ev[6]));
+    for (int k = 0; k < 3; k++) {
+      float a = 0, b = 0;
+      CK(cudaEventElapsedTime(&a, ev[2 * k], ev[1 + 2 * k]));
+      CK(cudaEventElapsedTime(&b, ev[1 + 2 * k], ev[2 + 2 * k]));
+      tx += a;
+      tz += b;
+    }
+    e->launches += 6;
+    cur = 1 - cur;
+  }
+  for (sf_solver* m : e->members) m->cur = cur;
+  for (cudaEvent_t& x : ev) cudaEventDestroy(x);
+  *ms_x = tx / (3.0 * nsteps);
+  *ms_z = tz / (3.0 * nsteps);
+  return SF_OK;
+}
+
+int sf_ensemble_synchronize(sf_ensemble* e) {
+  if (!e) return fail(SF_EINVAL, "null ensemble");
+  CK(cudaStreamSynchronize(e->st));
+  return SF_OK;
+}
+
+int sf_ensemble_launch_count(sf_ensemble* e, long long* count) {
+  if (!e || !count) return fail(SF_EINVAL, "bad argument");
+  *count = e->launches;
+  return SF_OK;
+}
+
+int sf_ensemble_stream(sf_ensemble* e, void** stream) {
+  if (!e || !stream) return fail(SF_EINVAL, "bad argument");
+  *stream = (void*)e->st;
   return SF_OK;
 }
 
