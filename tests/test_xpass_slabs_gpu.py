@@ -51,3 +51,33 @@ def test_slabs_per_block_do_not_change_the_step(name, nrun, mode, slabs):
         for f in range(5):
             tol = 5e-4 if f == 4 else 1e-5
             assert rel_l2(many[r, f], one[r, f]) < tol, (r, f, rel_l2(many[r, f], one[r, f]))
+
+
+@pytest.mark.parametrize("name,nrun,mode,bands", [
+    ("shear3d_small", 1, "nonlinear", 3),
+    ("shear3d_small", 2, "nonlinear", 8),
+    ("shear3d_small", 1, "linear", 2),
+    ("shear3d", 1, "nonlinear", 4),
+])
+def test_xy_bands_give_the_same_step_bit_for_bit(name, nrun, mode, bands):
+    """The banded 3D x-y pass (y transforms of other bands on side streams)
+    runs every block and column exactly as the one-band pass does, so the
+    step is bit-identical; the band count is a launch setting only."""
+    def run(b):
+        cfg = CONFIGS[name]
+        s = gpu_solver(cfg, nrun=nrun)
+        s.set_xy_bands(b)
+        for r in range(nrun):
+            s.set_state(r, make_ic(cfg, seed=500 + r))
+        if mode == "linear":
+            base = make_ic(cfg, seed=599, amp=5e-2)
+            for r in range(nrun):
+                s.SetBase(r, base["u1"], base["u2"], base["u3"], base["b"])
+        s.Prepare()
+        (s.TimeStepLinear if mode == "linear" else s.TimeStep)(3)
+        s.synchronize()
+        out = s.get_state_kept()
+        s.close()
+        return out
+    one, many = run(1), run(bands)
+    assert np.array_equal(one, many)
