@@ -720,6 +720,7 @@ def profile_only(args, s):
         t0 = time.perf_counter()
         for _ in range(max(1, args.steps)):
             net.forward(x)
+            net.set_data(x, y)   # a forward pass replaces the training inputs
             net.gradient()
         torch.cuda.synchronize()
         print(f"net forward + gradient {1e3 * (time.perf_counter() - t0) / max(1, args.steps):.3f} ms")

@@ -70,6 +70,10 @@ __host__ __device__ __forceinline__ int adj_row(int p, int s, int S) {
 __host__ __device__ inline int adj_rows(int S) { return adj_row(Q_COUNT - 1, S, S) + 1; }
 
 constexpr int kAdjGroups = 8;
+// lane groups of the 3D adjoint x pass: its 20 nodal rows leave room for one
+// block per SM, so the block carries more groups (24 x 16 lanes at N1 = 256)
+// to keep enough warps resident
+constexpr int kAdj3Groups = 24;
 inline int adiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 struct AdjLayout {
@@ -378,7 +382,7 @@ __host__ __device__ inline AdjLayout adj3_layout(int S, int N1, int K1, int bufs
   const size_t stg = sizeof(float2) * (size_t)12 * NS * K1, hat = sizeof(float2) * (size_t)adj3_rows(S) * K1;
   L.stg_off = off; off += stg > hat ? stg : hat;
   L.nod_off = off; off += sizeof(float) * (size_t)T_COUNT * NS * N1;
-  L.buf_off = off; off += sizeof(float2) * (size_t)kAdjGroups * bufstride;
+  L.buf_off = off; off += sizeof(float2) * (size_t)kAdj3Groups * bufstride;
   L.avg_off = off; off += sizeof(float) * (size_t)2 * NS;
   L.bytes = off;
   return L;
@@ -388,9 +392,9 @@ __host__ __device__ inline AdjLayout adj3_layout(int S, int N1, int K1, int bufs
 // 16 products and the 8 combinations of the forward 3D pass (C_f, C_fy with
 // r_f = Fy(C_f) + i ky Fy(C_fy)), into a.mixout
 template <int N1>
-__global__ void __launch_bounds__(kAdjGroups * 32) k_xpass_adj3(StageArgs a, int S) {
+__global__ void __launch_bounds__(kAdj3Groups * FFTShape<N1>::G) k_xpass_adj3(StageArgs a, int S) {
   constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, BUF = fft_buf_stride<N1>();
-  constexpr int NGB = kAdjGroups;
+  constexpr int NGB = kAdj3Groups;
   const Geo g = a.g;
   extern __shared__ __align__(16) unsigned char xsm[];
   const AdjLayout L = adj3_layout(S, N1, g.K1, BUF);
@@ -597,7 +601,7 @@ void adj3_launch(const StageArgs& a, cudaStream_t st) {
   constexpr int G = FFTShape<N1>::G, BUF = fft_buf_stride<N1>();
   int S = 2;
   while (S > 1 && adj3_layout(S, N1, g.K1, BUF).bytes > 227 * 1024) S--;
-  k_xpass_adj3<N1><<<dim3(adiv(g.N3, S), g.N2, g.nrun), kAdjGroups * G, adj3_layout(S, N1, g.K1, BUF).bytes, st>>>(
+  k_xpass_adj3<N1><<<dim3(adiv(g.N3, S), g.N2, g.nrun), kAdj3Groups * G, adj3_layout(S, N1, g.K1, BUF).bytes, st>>>(
       a, S);
 }
 

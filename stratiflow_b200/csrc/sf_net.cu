@@ -12,8 +12,8 @@
 //   forward          m = co, n = (b,z),        k = (tap,ci)
 //   backward data    m = ci, n = (b,z),        k = (tap,co)
 //   backward weights m = co, n = (tap,ci),     k = (b,z)
-// tiled 64 x 64 x 32 through shared memory, with warp tiles of 32 x 32 issued
-// as mma.sync m16n8k16 (bf16 x bf16 -> f32).
+// issued as tcgen05.mma on 128 x 128 tiles with the accumulator in tensor
+// memory (k_conv_gemm_tc).
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -29,8 +29,6 @@ extern void sf_set_error_message(const std::string& msg);
 namespace {
 
 constexpr int kTaps = 5, kPad = 2;
-constexpr int BM = 64, BN = 64, BK = 32, SK = BK + 8;   // shared rows padded by 16 bytes
-constexpr int kGemmThreads = 128;
 
 enum GemmMode { G_FWD = 0, G_BWD_DATA = 1, G_BWD_W = 2 };
 
@@ -48,117 +46,234 @@ struct ConvGemm {
   const __nv_bfloat16* mask; // backward data: keep where mask > 0 (ReLU')
 };
 
-__device__ __forceinline__ __nv_bfloat16 a_at(const ConvGemm& p, int m, int k) {
-  const __nv_bfloat16 zero = __float2bfloat16(0.f);
-  if (m >= p.M || k >= p.K) return zero;
-  switch (p.mode) {
-    case G_FWD: return p.W[(size_t)m * p.K + k];
-    case G_BWD_DATA: {
-      const int tap = k / p.Cout, co = k - tap * p.Cout;
-      return p.W[((size_t)co * kTaps + tap) * p.Cin + m];
-    }
-    default: return p.dP[(size_t)k * p.Cout + m];
+// ---------------------------------------------------------------- tcgen05 --
+// The implicit GEMMs on the 5th-generation tensor cores: a CTA of four
+// warps computes a 128 x 128 tile of C with tcgen05.mma (kind::f16, BF16 x
+// BF16 -> FP32) issued by one thread, the accumulator in tensor memory (128
+// lanes x 128 FP32 columns), A and B staged in shared memory as 64-wide K
+// slices in the canonical K-major layout without swizzling: 8-row x 16-byte
+// core matrices, the row groups 128 bytes apart (SBO) and the two 8-element
+// K halves of one instruction's K = 16 a whole row-group column apart (LBO).
+// Two shared-memory stages: the loads of K slice t + 1 overlap the MMAs of
+// slice t, and an mbarrier that the MMAs' commit arrives on frees a stage.
+// Every wait is bounded; a wait that runs out sets *err and the block skips
+// to freeing its tensor memory.
+constexpr int TM = 128, TN = 128, TK = 64, kTcThreads = 128;
+constexpr int kTcStageElems = (TM + TN) * TK;                      // bf16 per stage
+constexpr size_t kTcSmem = sizeof(__nv_bfloat16) * 2 * kTcStageElems;   // 64 KB
+constexpr long long kTcSpin = 1ll << 26;                           // bounded mbarrier waits
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major SWIZZLE_NONE shared-memory matrix descriptor (sm_100): start
+// address, leading (K) and stride (M/N) byte offsets in 16-byte units,
+// descriptor version 1
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major,
+// N and M of the instruction
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+  const uint32_t a = smem_u32(bar);
+  for (long long i = 0; i < kTcSpin; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(phase)
+        : "memory");
+    if (done) return true;
   }
+  return false;
 }
 
-__device__ __forceinline__ __nv_bfloat16 b_at(const ConvGemm& p, int n, int k) {
-  const __nv_bfloat16 zero = __float2bfloat16(0.f);
-  if (n >= p.N || k >= p.K) return zero;
-  switch (p.mode) {
-    case G_FWD: {
-      const int b = n / p.Z, z = n - b * p.Z, tap = k / p.Cin, ci = k - tap * p.Cin, zz = z + tap - kPad;
-      return (zz < 0 || zz >= p.Z) ? zero : p.X[((size_t)b * p.Z + zz) * p.Cin + ci];
-    }
-    case G_BWD_DATA: {
-      const int b = n / p.Z, z = n - b * p.Z, tap = k / p.Cout, co = k - tap * p.Cout, zz = z - tap + kPad;
-      return (zz < 0 || zz >= p.Z) ? zero : p.dP[((size_t)b * p.Z + zz) * p.Cout + co];
-    }
-    default: {
-      const int tap = n / p.Cin, ci = n - tap * p.Cin, b = k / p.Z, z = k - b * p.Z, zz = z + tap - kPad;
-      return (zz < 0 || zz >= p.Z) ? zero : p.X[((size_t)b * p.Z + zz) * p.Cin + ci];
-    }
+// 8 consecutive BF16 operands as one 16-byte load, zeros outside the matrix.
+// Channel counts are multiples of 8, so a run of 8 along the contiguous index
+// never crosses a tap or a row, and every run starts on a 16-byte boundary.
+__device__ __forceinline__ uint4 ld8(const __nv_bfloat16* p) { return *reinterpret_cast<const uint4*>(p); }
+__device__ __forceinline__ uint4 zero8() { return make_uint4(0u, 0u, 0u, 0u); }
+
+// A(m, k..k+7) where k is contiguous (forward: W[m][k])
+__device__ __forceinline__ uint4 a_k8(const ConvGemm& p, int m, int k) {
+  return (m < p.M && k < p.K) ? ld8(p.W + (size_t)m * p.K + k) : zero8();
+}
+// A(m..m+7, k) where m is contiguous (backward data: W[co][tap][m];
+// backward weights: dP[k][m])
+__device__ __forceinline__ uint4 a_m8(const ConvGemm& p, int m, int k) {
+  if (m >= p.M || k >= p.K) return zero8();
+  if (p.mode == G_BWD_DATA) {
+    const int tap = k / p.Cout, co = k - tap * p.Cout;
+    return ld8(p.W + ((size_t)co * kTaps + tap) * p.Cin + m);
   }
+  return ld8(p.dP + (size_t)k * p.Cout + m);
+}
+// B(n, k..k+7) where k is contiguous (forward: X rows; backward data: dP rows)
+__device__ __forceinline__ uint4 b_k8(const ConvGemm& p, int n, int k) {
+  if (n >= p.N || k >= p.K) return zero8();
+  const int b = n / p.Z, z = n - b * p.Z;
+  if (p.mode == G_FWD) {
+    const int tap = k / p.Cin, ci = k - tap * p.Cin, zz = z + tap - kPad;
+    return (zz < 0 || zz >= p.Z) ? zero8() : ld8(p.X + ((size_t)b * p.Z + zz) * p.Cin + ci);
+  }
+  const int tap = k / p.Cout, co = k - tap * p.Cout, zz = z - tap + kPad;
+  return (zz < 0 || zz >= p.Z) ? zero8() : ld8(p.dP + ((size_t)b * p.Z + zz) * p.Cout + co);
+}
+// B(n..n+7, k) where n is contiguous (backward weights: X rows at z + tap)
+__device__ __forceinline__ uint4 b_n8(const ConvGemm& p, int n, int k) {
+  if (n >= p.N || k >= p.K) return zero8();
+  const int tap = n / p.Cin, ci = n - tap * p.Cin, b = k / p.Z, z = k - b * p.Z, zz = z + tap - kPad;
+  return (zz < 0 || zz >= p.Z) ? zero8() : ld8(p.X + ((size_t)b * p.Z + zz) * p.Cin + ci);
 }
 
-__device__ __forceinline__ void mma_bf16(float (&c)[4], const unsigned (&a)[4], const unsigned (&b)[2]) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+// element of shared tile [rows][TK] at (r, c) in the core-matrix layout:
+// core (row group r/8, K chunk c/8) at ((c/8) * rows/8 + r/8) * 64 elements
+template <int ROWS>
+__device__ __forceinline__ int tc_off(int r, int c) {
+  return (((c >> 3) * (ROWS / 8) + (r >> 3)) << 6) + ((r & 7) << 3) + (c & 7);
 }
 
-// One 64 x 64 tile of C per block; 4 warps of 32 x 32
-__global__ void __launch_bounds__(kGemmThreads) k_conv_gemm(ConvGemm p) {
-  __shared__ __align__(16) __nv_bfloat16 As[BM][SK];
-  __shared__ __align__(16) __nv_bfloat16 Bs[BN][SK];
-  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+__global__ void __launch_bounds__(kTcThreads) k_conv_gemm_tc(ConvGemm p, int* err) {
+  extern __shared__ __align__(128) unsigned char tsm[];
+  __nv_bfloat16* stage0 = reinterpret_cast<__nv_bfloat16*>(tsm);
+  __shared__ __align__(8) uint64_t mbar[2];
+  __shared__ uint32_t tmem_base;
+  __shared__ int failed;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-  const int g = lane >> 2, t = lane & 3;
-  // which index runs fastest across threads when a tile is loaded: the one
-  // that is contiguous in memory for this operand
+  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
   const bool a_mfast = p.mode != G_FWD, b_nfast = p.mode == G_BWD_W;
-  float acc[2][4][4] = {};
-  for (int k0 = 0; k0 < p.K; k0 += BK) {
-    for (int i = tid; i < BM * BK; i += kGemmThreads) {
-      const int r = a_mfast ? i % BM : i / BK, c = a_mfast ? i / BM : i % BK;
-      As[r][c] = a_at(p, m0 + r, k0 + c);
-    }
-    for (int i = tid; i < BN * BK; i += kGemmThreads) {
-      const int r = b_nfast ? i % BN : i / BK, c = b_nfast ? i / BN : i % BK;
-      Bs[r][c] = b_at(p, n0 + r, k0 + c);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int kk = 0; kk < BK; kk += 16) {
-      unsigned af[2][4], bf[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; i++) {
-        const int r = wm + i * 16 + g;
-        af[i][0] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t]);
-        af[i][1] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t]);
-        af[i][2] = *reinterpret_cast<const unsigned*>(&As[r][kk + 2 * t + 8]);
-        af[i][3] = *reinterpret_cast<const unsigned*>(&As[r + 8][kk + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int c = wn + j * 8 + g;
-        bf[j][0] = *reinterpret_cast<const unsigned*>(&Bs[c][kk + 2 * t]);
-        bf[j][1] = *reinterpret_cast<const unsigned*>(&Bs[c][kk + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int i = 0; i < 2; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) mma_bf16(acc[i][j], af[i], bf[j]);
-    }
-    __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
-  // epilogue: c0,c1 at (row g, cols 2t, 2t+1), c2,c3 at (row g+8, ...)
+  if (tid == 0) {
+    failed = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = tmem_base;
+  const int nk = (p.K + TK - 1) / TK;
+  uint32_t phase[2] = {0, 0};
+  constexpr uint32_t idesc = umma_idesc_bf16(TM, TN);
+  for (int kt = 0; kt < nk && !failed; kt++) {
+    const int s = kt & 1, k0 = kt * TK;
+    __nv_bfloat16* As = stage0 + (size_t)s * kTcStageElems;
+    __nv_bfloat16* Bs = As + TM * TK;
+    if (kt >= 2) {   // the MMAs of slice kt - 2 read this stage
+      if (!mbar_wait(&mbar[s], phase[s])) {
+        if (tid == 0) { failed = 1; atomicExch(err, 1); }
+      }
+      phase[s] ^= 1;
+    }
+    __syncthreads();
+    if (failed) break;
+    // one 16-byte load per thread and pass: a core-matrix row when K is the
+    // contiguous index, else 8 rows of one K column
+    if (!a_mfast) {
+      for (int i = tid; i < TM * (TK / 8); i += kTcThreads) {
+        const int r = i / (TK / 8), c = 8 * (i % (TK / 8));
+        *reinterpret_cast<uint4*>(&As[tc_off<TM>(r, c)]) = a_k8(p, m0 + r, k0 + c);
+      }
+    } else {
+      for (int i = tid; i < (TM / 8) * TK; i += kTcThreads) {
+        const int r = 8 * (i % (TM / 8)), c = i / (TM / 8);
+        const uint4 v = a_m8(p, m0 + r, k0 + c);
+        const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-  for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 8; j++) As[tc_off<TM>(r + j, c)] = e[j];
+      }
+    }
+    if (!b_nfast) {
+      for (int i = tid; i < TN * (TK / 8); i += kTcThreads) {
+        const int r = i / (TK / 8), c = 8 * (i % (TK / 8));
+        *reinterpret_cast<uint4*>(&Bs[tc_off<TN>(r, c)]) = b_k8(p, n0 + r, k0 + c);
+      }
+    } else {
+      for (int i = tid; i < (TN / 8) * TK; i += kTcThreads) {
+        const int r = 8 * (i % (TN / 8)), c = i / (TN / 8);
+        const uint4 v = b_n8(p, n0 + r, k0 + c);
+        const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+        for (int j = 0; j < 8; j++) Bs[tc_off<TN>(r + j, c)] = e[j];
+      }
+    }
+    // the generic-proxy stores must be visible to the tensor cores' async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;");
+      const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int m = m0 + wm + i * 16 + g + (e >= 2 ? 8 : 0);
-        const int n = n0 + wn + j * 8 + 2 * t + (e & 1);
-        if (m >= p.M || n >= p.N) continue;
-        float v = acc[i][j][e];
+      for (int kk = 0; kk < TK / 16; kk++) {
+        // K = 16 per instruction: K chunks 2kk and 2kk + 1
+        const uint64_t da = umma_desc(a0 + kk * 2 * (TM / 8) * 128, (TM / 8) * 128, 128);
+        const uint64_t db = umma_desc(b0 + kk * 2 * (TN / 8) * 128, (TN / 8) * 128, 128);
+        const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&mbar[s]))
+                   : "memory");
+    }
+  }
+  // the last commit covers every MMA issued before it
+  if (!failed && nk > 0) {
+    const int s = (nk - 1) & 1;
+    if (!mbar_wait(&mbar[s], phase[s]) && tid == 0) { failed = 1; atomicExch(err, 1); }
+  }
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  if (!failed) {
+    // warp w reads tensor-memory lanes 32w..32w+31: row m0 + 32w + lane
+    const int m = m0 + 32 * warp + lane;
+    for (int c = 0; c < TN; c += 8) {
+      uint32_t v[8];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+          : "r"(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m >= p.M) continue;
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int n = n0 + c + e;
+        if (n >= p.N) break;
+        float x = __uint_as_float(v[e]);
         if (p.mode == G_FWD) {
-          v += p.bias[m];
+          x += p.bias[m];
           const size_t o = (size_t)n * p.M + m;
-          if (p.outF) p.outF[o] = v;
-          if (p.outB) p.outB[o] = __float2bfloat16(p.relu ? fmaxf(v, 0.f) : v);
+          if (p.outF) p.outF[o] = x;
+          if (p.outB) p.outB[o] = __float2bfloat16(p.relu ? fmaxf(x, 0.f) : x);
         } else if (p.mode == G_BWD_DATA) {
           const size_t o = (size_t)n * p.M + m;
-          if (p.mask && !(__bfloat162float(p.mask[o]) > 0.f)) v = 0.f;
-          if (p.outF) p.outF[o] = v;
-          if (p.outB) p.outB[o] = __float2bfloat16(v);
+          if (p.mask && !(__bfloat162float(p.mask[o]) > 0.f)) x = 0.f;
+          if (p.outF) p.outF[o] = x;
+          if (p.outB) p.outB[o] = __float2bfloat16(x);
         } else {
-          p.outF[(size_t)m * p.N + n] = v;
+          p.outF[(size_t)m * p.N + n] = x;
         }
       }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
 }
 
 __global__ void k_to_bf16(const float* __restrict__ x, __nv_bfloat16* __restrict__ y, size_t n) {
@@ -233,6 +348,7 @@ struct sf_net {
   double* loss = nullptr;
   long long t = 0;                   // Adam steps taken
   cudaStream_t st = nullptr;
+  int* err = nullptr;                // set by a GEMM block whose bounded wait ran out
 };
 
 namespace {
@@ -254,8 +370,8 @@ int gemm(sf_net* n, ConvGemm p) {
     case G_BWD_DATA: p.M = p.Cin; p.N = p.B * p.Z; p.K = kTaps * p.Cout; break;
     default: p.M = p.Cout; p.N = kTaps * p.Cin; p.K = p.B * p.Z; break;
   }
-  dim3 grid((p.N + BN - 1) / BN, (p.M + BM - 1) / BM);
-  k_conv_gemm<<<grid, kGemmThreads, 0, n->st>>>(p);
+  dim3 grid((p.N + TN - 1) / TN, (p.M + TM - 1) / TM);
+  k_conv_gemm_tc<<<grid, kTcThreads, kTcSmem, n->st>>>(p, n->err);
   NCK(cudaGetLastError());
   return SF_OK;
 }
@@ -327,6 +443,17 @@ int upload_input(sf_net* n, const float* x, int B) {
 
 extern "C" {
 
+// after a synchronisation: a GEMM whose tensor-core wait ran out is an error
+static int net_status(sf_net* n) {
+  int h = 0;
+  NCK(cudaMemcpy(&h, n->err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    NCK(cudaMemset(n->err, 0, sizeof(int)));
+    return nfail(SF_ECUDA, "a tensor-core GEMM block gave up waiting for its MMAs");
+  }
+  return SF_OK;
+}
+
 int sf_net_create(int nlayers, const int* channels, int Z, int max_batch, unsigned long long seed, void* stream,
                   sf_net** out) {
   if (!out || nlayers < 1 || nlayers > 16 || !channels || Z < 1 || max_batch < 1)
@@ -374,6 +501,12 @@ int sf_net_create(int nlayers, const int* channels, int Z, int max_batch, unsign
   if (cudaMalloc(&n->tgt, sizeof(float) * rows * n->ch[nlayers]) != cudaSuccess) return bail("cudaMalloc targets");
   if (cudaMalloc(&n->xin, sizeof(float) * rows * n->ch[0]) != cudaSuccess) return bail("cudaMalloc input");
   if (cudaMalloc(&n->loss, sizeof(double)) != cudaSuccess) return bail("cudaMalloc loss");
+  if (cudaMalloc(&n->err, sizeof(int)) != cudaSuccess) return bail("cudaMalloc status");
+  if (cudaMemset(n->err, 0, sizeof(int)) != cudaSuccess ||
+      cudaFuncSetAttribute(k_conv_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem) != cudaSuccess) {
+    sf_net_destroy(n);
+    return nfail(SF_ECUDA, "setting up the tensor-core GEMM");
+  }
   if (cudaMemcpy(n->w, h.data(), sizeof(float) * n->nparam, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(n->m1, 0, sizeof(float) * n->nparam) != cudaSuccess ||
       cudaMemset(n->m2, 0, sizeof(float) * n->nparam) != cudaSuccess ||
@@ -395,7 +528,7 @@ int sf_net_destroy(sf_net* n) {
   for (auto p : n->act) cudaFree(p);
   for (auto p : n->dP) cudaFree(p);
   for (void* p : {(void*)n->w, (void*)n->gr, (void*)n->m1, (void*)n->m2, (void*)n->wb, (void*)n->out,
-                  (void*)n->tgt, (void*)n->xin, (void*)n->loss})
+                  (void*)n->tgt, (void*)n->xin, (void*)n->loss, (void*)n->err})
     cudaFree(p);
   delete n;
   return SF_OK;
@@ -434,7 +567,7 @@ int sf_net_forward(sf_net* n, const float* x, int batch, float* y) {
   n->nb_data = 0;   // act[0] no longer holds the training inputs
   NCK(cudaMemcpyAsync(y, n->out, sizeof(float) * batch * n->Z * n->ch[n->nl], cudaMemcpyDeviceToHost, n->st));
   NCK(cudaStreamSynchronize(n->st));
-  return SF_OK;
+  return net_status(n);
 }
 
 int sf_net_set_data(sf_net* n, const float* x, const float* target, int batch) {
@@ -455,7 +588,7 @@ int sf_net_gradient(sf_net* n, float* grad, double* loss) {
   if (grad) NCK(cudaMemcpyAsync(grad, n->gr, sizeof(float) * n->nparam, cudaMemcpyDeviceToHost, n->st));
   if (loss) NCK(cudaMemcpyAsync(loss, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->st));
   NCK(cudaStreamSynchronize(n->st));
-  return SF_OK;
+  return net_status(n);
 }
 
 int sf_net_train(sf_net* n, int steps, double lr, double* losses) {
@@ -475,7 +608,7 @@ int sf_net_train(sf_net* n, int steps, double lr, double* losses) {
     if (losses) NCK(cudaMemcpyAsync(losses + s, n->loss, sizeof(double), cudaMemcpyDeviceToHost, n->st));
   }
   NCK(cudaStreamSynchronize(n->st));
-  return SF_OK;
+  return net_status(n);
 }
 
 }  // extern "C"

@@ -51,7 +51,10 @@ def test_dropin_fixed_evolve_matches_python_and_oracle(tmp_path):
     n = int(np.prod(shape))
     f = np.frombuffer(raw[:5 * n * 8], dtype=np.complex64).reshape(5, *shape)
     ke, pe = np.frombuffer(raw[5 * n * 8:], dtype=np.float64)
-    s = gpu_solver(cfg)
+    # the drop-in keeps deltaT in stratifloat (float), as IMEXRK.h does; the
+    # Python path gets the same float-rounded step (p, which accumulates q/h,
+    # would otherwise differ by the last bit of h amplified ~1000 times)
+    s = gpu_solver(dict(cfg, dt=float(np.float32(cfg["dt"]))))
     s.set_state(0, ic)
     s.Prepare()
     s.TimeStep(10)
