@@ -664,7 +664,7 @@ def run_ensemble3(args, wl, ws, rank, dist, local):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded tanh shear layers, 1e-3 perturbations)",
         "config": {"workload": f"ensemble3: {len(runs)} independent 2D runs, N1 in {{64,128,256}}, "
                                f"N3 in {{128,256,384}}, Ri in [0.05,0.25] (seed {wl['seed']}), Re {wl['Re']:g}, "
-                               f"Pr {wl['Pr']:g}, dt {wl['dt']:g}, one x-pass and one z-solve launch per RK stage",
+                               f"Pr {wl['Pr']:g}, dt {wl['dt']:g}, one launch per RK stage (persistent blocks over x-pass then z-solve work items)",
                    "grids": grids, "parallelism": f"replicas x{args.gpus}",
                    "l2": "L2-resident working set (launch-bound case)"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": dom_bytes / (dom_ms / 1e3) / 1e9, "peak": hbm,

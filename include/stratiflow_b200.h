@@ -245,8 +245,8 @@ int sf_remove_divergence_noalloc(const sf_grid* grid, const sf_flow* flow, doubl
  * (sf_ensemble_member) that takes every single-solver call: sf_set_ri,
  * sf_set_background, sf_set_field / sf_get_field, sf_prepare, sf_energy, ...
  * sf_ensemble_step advances every member by nsteps IMEXRK::TimeStep
- * (IMEXRK.cpp:8-24) with one x-pass launch and one z-solve launch per RK stage
- * over all members' work items (one CUDA graph per step); it waits for the
+ * (IMEXRK.cpp:8-24) with one launch per RK stage over all members' x-pass
+ * and z-solve work items (one CUDA graph per step); it waits for the
  * members' own queued work first and returns without waiting for the steps:
  * call sf_ensemble_synchronize before using a member again. Members must not
  * be stepped on their own in between (sf_ensemble_step then reports

@@ -468,8 +468,8 @@ class IMEXRK:
 
 class Ensemble:
     """Independent 2D runs on grids of different sizes stepped together
-    (sf_ensemble_*): one x-pass launch and one z-solve launch per RK stage
-    over every run's work items, one CUDA graph per step. grids is a list of
+    (sf_ensemble_*): one launch per RK stage over every run's x-pass and
+    z-solve work items, one CUDA graph per step. grids is a list of
     (N1, N3); flows a list of (L1, L3, Re, Pr) or one tuple for all; dt one
     value or a list. members[r] is an IMEXRK view of run r (set_ri,
     SetBackground, set_state, Prepare, get_field, energy, ...)."""

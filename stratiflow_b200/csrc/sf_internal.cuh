@@ -133,6 +133,12 @@ size_t ensemble_zstep_smem(int N3);
 int launch_xpass_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st);
 int launch_zstep_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st);
 int prepare_ensemble_kernels();
+// the whole stage in one launch of `blocks` persistent blocks over work-item
+// counters (counters[0] the next item, counters[1 + r] member r's finished
+// x-pass items; cleared before each step)
+int launch_ens_stage(const StageArgs* args, const EnsItem* xitems, int nx, const EnsItem* zitems, int nz,
+                     int* counters, const int* xneed, int* err, int blocks, size_t smem, cudaStream_t st);
+int ensemble_stage_blocks(size_t smem);
 int launch_grad_sq(const Geo& g, const float2* S, int nruns, const float* zc, const double* kxd, const double* kyd,
                    double* out, cudaStream_t st);
 int launch_base_nodal(const Geo& g, const float2* kept_modal, int field, float* base_out,

@@ -1017,6 +1017,86 @@ __global__ void __launch_bounds__(kEnsThreads, 2) k_zstep_ens(const StageArgs* _
 }
 
 
+// One RK stage of every member in one launch: blocks claim work items from
+// counters[0] in order, all x-pass items first (largest members first), then
+// all z-step items. A z-step item of member r starts once member r's x-pass
+// items have all finished (counters[1 + r] reaches xneed[r]). A block claims
+// its next item as it starts the current one, so the claim's latency hides
+// behind the work; every wait still ends: an item claimed ahead always has a
+// higher index than the claiming block's current item, so every x-pass item
+// is being run or is next after an x-pass item being run, and x-pass items
+// wait on nothing. The waits are bounded all the same: one that runs out
+// sets *err and skips its item. The host clears the counters before each step.
+constexpr long long kEnsSpin = 1ll << 24;   // x 64 ns: about a second
+
+__global__ void __launch_bounds__(kEnsThreads, 2) k_ens_stage(const StageArgs* __restrict__ args,
+                                                              const EnsItem* __restrict__ xitems, int nx,
+                                                              const EnsItem* __restrict__ zitems, int nz,
+                                                              int* counters, const int* __restrict__ xneed,
+                                                              int* err) {
+  __shared__ __align__(16) StageArgs sa;
+  __shared__ int next, have, ok;
+  static_assert(sizeof(StageArgs) % sizeof(int) == 0, "StageArgs copied as words");
+  if (threadIdx.x == 0) {
+    next = atomicAdd(&counters[0], 1);
+    have = -1;
+  }
+  __syncthreads();
+  for (;;) {
+    const int i = next;
+    if (i >= nx + nz) break;
+    const bool xp = i < nx;
+    const EnsItem it = xp ? xitems[i] : zitems[i - nx];
+    const bool fresh = it.run != have;
+    __syncthreads();   // everyone has read next and have
+    if (threadIdx.x == 0) {
+      next = atomicAdd(&counters[0], 1);
+      have = it.run;
+      ok = 1;
+    }
+    if (fresh) {   // this member's stage arguments, copied by the block's threads
+      const int* src = reinterpret_cast<const int*>(args + it.run);
+      int* dst = reinterpret_cast<int*>(&sa);
+      for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / sizeof(int)); w += blockDim.x) dst[w] = src[w];
+    }
+    if (!xp && threadIdx.x == 0) {
+      const volatile int* done = counters + 1 + it.run;
+      long long n = 0;
+      while (*done < xneed[it.run] && n < kEnsSpin) {
+        __nanosleep(64);
+        n++;
+      }
+      if (*done < xneed[it.run]) {
+        ok = 0;
+        atomicExch(err, 1);
+      }
+      __threadfence();   // the member's x-pass results before its z step reads them
+    }
+    __syncthreads();
+    if (xp) {
+      switch (sa.g.N1) {
+        case 16: xpass_body<16, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        case 32: xpass_body<32, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        case 64: xpass_body<64, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        case 128: xpass_body<128, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        case 256: xpass_body<256, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        case 512: xpass_body<512, false>(sa, it.S, it.iters, it.x, 0, 0); break;
+        default: break;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        __threadfence();   // this item's r rows, before it counts as done
+        atomicAdd(&counters[1 + it.run], 1);
+      }
+    } else if (ok) {
+      if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
+      else z_step_body<8, false>(sa, it.x, 0);
+    }
+    __syncthreads();
+  }
+}
+
+
 // ====================================================== factorisation ====
 // Thomas factors of every (factor set, mode) in FP64 (Tridiagonal.h:14-27):
 // inv_den_j = 1/(b_j - a_j C_{j-1}), stored as float. Rows follow
@@ -1507,10 +1587,24 @@ int launch_zstep_ens(const StageArgs* args, const EnsItem* items, int nitems, si
   k_zstep_ens<<<nitems, kEnsThreads, smem, st>>>(args, items);
   return 1;
 }
+int launch_ens_stage(const StageArgs* args, const EnsItem* xitems, int nx, const EnsItem* zitems, int nz,
+                     int* counters, const int* xneed, int* err, int blocks, size_t smem, cudaStream_t st) {
+  k_ens_stage<<<blocks, kEnsThreads, smem, st>>>(args, xitems, nx, zitems, nz, counters, xneed, err);
+  return 1;
+}
+int ensemble_stage_blocks(size_t smem) {
+  int per_sm = 0, sms = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_ens_stage, kEnsThreads, smem) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return (per_sm < 1 ? 1 : per_sm) * sms;
+}
 int prepare_ensemble_kernels() {
   const int lim = 227 * 1024 - (int)sizeof(StageArgs) - 64;
   cudaError_t e = cudaFuncSetAttribute(k_xpass_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zstep_ens, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ens_stage, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   return e == cudaSuccess ? 0 : -1;
 }
 

@@ -51,26 +51,31 @@ struct ConvGemm {
 // warps computes a 128 x 128 tile of C with tcgen05.mma (kind::f16, BF16 x
 // BF16 -> FP32) issued by one thread, the accumulator in tensor memory (128
 // lanes x 128 FP32 columns), A and B staged in shared memory as 64-wide K
-// slices in the canonical K-major layout without swizzling: 8-row x 16-byte
-// core matrices, the row groups 128 bytes apart (SBO) and the two 8-element
-// K halves of one instruction's K = 16 a whole row-group column apart (LBO).
+// slices in the K-major layout with the 128-byte swizzle: each row's 64
+// elements are one 128-byte line whose 16-byte chunk c sits at c ^ (row % 8),
+// 8-row groups 1024 bytes apart (SBO); an instruction's K = 16 is the next 32
+// bytes of every row (the descriptor's start address advances by 32 bytes).
+// The 16-byte operand loads of one row then fill one line without bank
+// conflicts.
 // Two shared-memory stages: the loads of K slice t + 1 overlap the MMAs of
 // slice t, and an mbarrier that the MMAs' commit arrives on frees a stage.
 // Every wait is bounded; a wait that runs out sets *err and the block skips
 // to freeing its tensor memory.
 constexpr int TM = 128, TN = 128, TK = 64, kTcThreads = 128;
 constexpr int kTcStageElems = (TM + TN) * TK;                      // bf16 per stage
-constexpr size_t kTcSmem = sizeof(__nv_bfloat16) * 2 * kTcStageElems;   // 64 KB
+// two stages, plus room to align the first to the swizzle's 1024-byte period
+constexpr size_t kTcSmem = sizeof(__nv_bfloat16) * 2 * kTcStageElems + 1024;
 constexpr long long kTcSpin = 1ll << 26;                           // bounded mbarrier waits
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// K-major SWIZZLE_NONE shared-memory matrix descriptor (sm_100): start
-// address, leading (K) and stride (M/N) byte offsets in 16-byte units,
-// descriptor version 1
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+// K-major shared-memory matrix descriptor (sm_100) of the 128-byte swizzle:
+// start address and the byte offsets in 16-byte units (LBO 16 bytes, unused
+// by this layout; SBO 1024 bytes between 8-row groups), descriptor version 1,
+// layout type 2 (SWIZZLE_128B)
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+         (2ull << 61);
 }
 
 // instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major,
@@ -133,16 +138,15 @@ __device__ __forceinline__ uint4 b_n8(const ConvGemm& p, int n, int k) {
   return (zz < 0 || zz >= p.Z) ? zero8() : ld8(p.X + ((size_t)b * p.Z + zz) * p.Cin + ci);
 }
 
-// element of shared tile [rows][TK] at (r, c) in the core-matrix layout:
-// core (row group r/8, K chunk c/8) at ((c/8) * rows/8 + r/8) * 64 elements
-template <int ROWS>
+// element (r, c) of a [rows][TK = 64] tile in the 128-byte-swizzled layout
 __device__ __forceinline__ int tc_off(int r, int c) {
-  return (((c >> 3) * (ROWS / 8) + (r >> 3)) << 6) + ((r & 7) << 3) + (c & 7);
+  return ((r >> 3) << 9) + ((r & 7) << 6) + ((((c >> 3) ^ (r & 7))) << 3) + (c & 7);
 }
 
 __global__ void __launch_bounds__(kTcThreads) k_conv_gemm_tc(ConvGemm p, int* err) {
   extern __shared__ __align__(128) unsigned char tsm[];
-  __nv_bfloat16* stage0 = reinterpret_cast<__nv_bfloat16*>(tsm);
+  // the stages start on a 1024-byte boundary (the swizzle pattern's period)
+  __nv_bfloat16* stage0 = reinterpret_cast<__nv_bfloat16*>(tsm + ((1024 - (smem_u32(tsm) & 1023)) & 1023));
   __shared__ __align__(8) uint64_t mbar[2];
   __shared__ uint32_t tmem_base;
   __shared__ int failed;
@@ -181,32 +185,35 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_gemm_tc(ConvGemm p, int* er
     if (failed) break;
     // one 16-byte load per thread and pass: a core-matrix row when K is the
     // contiguous index, else 8 rows of one K column
+    // K contiguous: 8 threads load one row's 128 bytes and fill its line;
+    // M or N contiguous: a thread loads 8 rows of one K column, and the
+    // threads of a warp take consecutive columns (conflict-free stores)
     if (!a_mfast) {
       for (int i = tid; i < TM * (TK / 8); i += kTcThreads) {
         const int r = i / (TK / 8), c = 8 * (i % (TK / 8));
-        *reinterpret_cast<uint4*>(&As[tc_off<TM>(r, c)]) = a_k8(p, m0 + r, k0 + c);
+        *reinterpret_cast<uint4*>(&As[tc_off(r, c)]) = a_k8(p, m0 + r, k0 + c);
       }
     } else {
       for (int i = tid; i < (TM / 8) * TK; i += kTcThreads) {
-        const int r = 8 * (i % (TM / 8)), c = i / (TM / 8);
+        const int c = i % TK, r = 8 * (i / TK);
         const uint4 v = a_m8(p, m0 + r, k0 + c);
         const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-        for (int j = 0; j < 8; j++) As[tc_off<TM>(r + j, c)] = e[j];
+        for (int j = 0; j < 8; j++) As[tc_off(r + j, c)] = e[j];
       }
     }
     if (!b_nfast) {
       for (int i = tid; i < TN * (TK / 8); i += kTcThreads) {
         const int r = i / (TK / 8), c = 8 * (i % (TK / 8));
-        *reinterpret_cast<uint4*>(&Bs[tc_off<TN>(r, c)]) = b_k8(p, n0 + r, k0 + c);
+        *reinterpret_cast<uint4*>(&Bs[tc_off(r, c)]) = b_k8(p, n0 + r, k0 + c);
       }
     } else {
       for (int i = tid; i < (TN / 8) * TK; i += kTcThreads) {
-        const int r = 8 * (i % (TN / 8)), c = i / (TN / 8);
+        const int c = i % TK, r = 8 * (i / TK);
         const uint4 v = b_n8(p, n0 + r, k0 + c);
         const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(&v);
 #pragma unroll
-        for (int j = 0; j < 8; j++) Bs[tc_off<TN>(r + j, c)] = e[j];
+        for (int j = 0; j < 8; j++) Bs[tc_off(r + j, c)] = e[j];
       }
     }
     // the generic-proxy stores must be visible to the tensor cores' async proxy
@@ -217,9 +224,9 @@ __global__ void __launch_bounds__(kTcThreads) k_conv_gemm_tc(ConvGemm p, int* er
       const uint32_t a0 = smem_u32(As), b0 = smem_u32(Bs);
 #pragma unroll
       for (int kk = 0; kk < TK / 16; kk++) {
-        // K = 16 per instruction: K chunks 2kk and 2kk + 1
-        const uint64_t da = umma_desc(a0 + kk * 2 * (TM / 8) * 128, (TM / 8) * 128, 128);
-        const uint64_t db = umma_desc(b0 + kk * 2 * (TN / 8) * 128, (TN / 8) * 128, 128);
+        // K = 16 per instruction: bytes 32 kk .. 32 kk + 31 of every row
+        const uint64_t da = umma_desc_sw128(a0 + 32 * kk);
+        const uint64_t db = umma_desc_sw128(b0 + 32 * kk);
         const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

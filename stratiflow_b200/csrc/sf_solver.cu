@@ -882,8 +882,9 @@ int sf_launch_count(sf_solver* s, long long* count) {
 // ---------------------------------------------------------------- ensembles
 // A batch of independent 2D runs on grids of different sizes: one member
 // solver per run (its own buffers, factors, Ri and background), stepped
-// together with one x-pass launch and one z-step launch per RK stage over the
-// work items of every member, captured as one CUDA graph per step parity.
+// together with one launch per RK stage over the work items of every member
+// (k_ens_stage: every member's x-pass blocks, then its z-step blocks), captured
+// as one CUDA graph per step parity.
 struct sf_ensemble {
   int device = 0;
   std::vector<sf_solver*> members;
@@ -893,6 +894,10 @@ struct sf_ensemble {
   EnsItem *d_x = nullptr, *d_z = nullptr;
   int nx = 0, nz = 0;
   size_t xsmem = 0, zsmem = 0;
+  int* d_counters = nullptr;   // [3 stages][1 + nrun] work-item counters of the stage launches
+  int* d_xneed = nullptr;      // [nrun] x-pass items per member
+  int* d_err = nullptr;        // a z-step item whose wait ran out
+  int blocks = 0;              // persistent blocks of a stage launch
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   long long launches = 0;
 };
@@ -900,9 +905,9 @@ struct sf_ensemble {
 static void ens_free(sf_ensemble* e) {
   for (cudaGraphExec_t& gx : e->graph)
     if (gx) cudaGraphExecDestroy(gx);
-  if (e->d_args) cudaFree(e->d_args);
-  if (e->d_x) cudaFree(e->d_x);
-  if (e->d_z) cudaFree(e->d_z);
+  for (void* p : {(void*)e->d_args, (void*)e->d_x, (void*)e->d_z, (void*)e->d_counters, (void*)e->d_xneed,
+                  (void*)e->d_err})
+    if (p) cudaFree(p);
   if (e->st) cudaStreamDestroy(e->st);
   for (sf_solver* m : e->members)
     if (m) sf_destroy(m);
@@ -939,9 +944,11 @@ int sf_ensemble_create(int nrun, const sf_grid* grids, const sf_flow* flows, con
     return (long long)grids[a].N1 * grids[a].N3 > (long long)grids[b].N1 * grids[b].N3;
   });
   std::vector<EnsItem> xi, zi;
+  std::vector<int> xneed(nrun, 0);
   for (int r : order) {
     const Geo& g = e->members[r]->g;
     const int S = 4;
+    xneed[r] = (g.N3 + S - 1) / S;
     for (int c = 0; c < (g.N3 + S - 1) / S; c++) xi.push_back(EnsItem{r, c, S, 1});
     for (int q = 0; q < (g.P + 15) / 16; q++) zi.push_back(EnsItem{r, q, 0, 0});
     e->xsmem = std::max(e->xsmem, ensemble_xpass_smem(g.N1, S));
@@ -955,11 +962,17 @@ int sf_ensemble_create(int nrun, const sf_grid* grids, const sf_flow* flows, con
   if (ce == cudaSuccess) ce = cudaMalloc(&e->d_args, sizeof(StageArgs) * 6 * nrun);
   if (ce == cudaSuccess) ce = cudaMemcpy(e->d_x, xi.data(), sizeof(EnsItem) * xi.size(), cudaMemcpyHostToDevice);
   if (ce == cudaSuccess) ce = cudaMemcpy(e->d_z, zi.data(), sizeof(EnsItem) * zi.size(), cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_counters, sizeof(int) * 3 * (nrun + 1));
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_xneed, sizeof(int) * nrun);
+  if (ce == cudaSuccess) ce = cudaMalloc(&e->d_err, sizeof(int));
+  if (ce == cudaSuccess) ce = cudaMemcpy(e->d_xneed, xneed.data(), sizeof(int) * nrun, cudaMemcpyHostToDevice);
+  if (ce == cudaSuccess) ce = cudaMemset(e->d_err, 0, sizeof(int));
   if (ce != cudaSuccess) {
     ens_free(e);
     return fail(ce == cudaErrorMemoryAllocation ? SF_ENOMEM : SF_ECUDA, std::string("ensemble: ") + cudaGetErrorString(ce));
   }
   e->h_args.resize((size_t)6 * nrun);
+  e->blocks = ensemble_stage_blocks(std::max(e->xsmem, e->zsmem));
   *out = e;
   return SF_OK;
 }
@@ -1004,10 +1017,11 @@ int sf_ensemble_step(sf_ensemble* e, int nsteps) {
     if (e->graph[p]) continue;
     cudaGraph_t gr;
     CK(cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(e->d_counters, 0, sizeof(int) * 3 * (R + 1), e->st);
     for (int k = 0; k < 3; k++) {
       const StageArgs* a = e->d_args + ((size_t)p * 3 + k) * R;
-      launch_xpass_ens(a, e->d_x, e->nx, e->xsmem, e->st);
-      launch_zstep_ens(a, e->d_z, e->nz, e->zsmem, e->st);
+      launch_ens_stage(a, e->d_x, e->nx, e->d_z, e->nz, e->d_counters + (size_t)k * (R + 1), e->d_xneed, e->d_err,
+                       e->blocks, std::max(e->xsmem, e->zsmem), e->st);
     }
     cudaError_t ce = cudaStreamEndCapture(e->st, &gr);
     if (ce != cudaSuccess) return fail(SF_ECUDA, std::string("ensemble graph capture: ") + cudaGetErrorString(ce));
@@ -1018,7 +1032,7 @@ int sf_ensemble_step(sf_ensemble* e, int nsteps) {
   int cur = par;
   for (int i = 0; i < nsteps; i++) {
     CK(cudaGraphLaunch(e->graph[cur], e->st));
-    e->launches += 6;
+    e->launches += 3;
     cur = 1 - cur;   // three stages flip the state buffer three times
   }
   for (sf_solver* m : e->members) m->cur = cur;
@@ -1066,6 +1080,12 @@ int sf_ensemble_profile(sf_ensemble* e, int nsteps, double* ms_x, double* ms_z) 
 int sf_ensemble_synchronize(sf_ensemble* e) {
   if (!e) return fail(SF_EINVAL, "null ensemble");
   CK(cudaStreamSynchronize(e->st));
+  int h = 0;
+  CK(cudaMemcpy(&h, e->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) {
+    CK(cudaMemset(e->d_err, 0, sizeof(int)));
+    return fail(SF_ECUDA, "an ensemble z-step item gave up waiting for its member's x pass");
+  }
   return SF_OK;
 }
 
