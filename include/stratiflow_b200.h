@@ -192,6 +192,13 @@ int sf_set_xy_bands(sf_solver* s, int bands);
  * rounding (the chunked solve reassociates the recurrence). */
 int sf_set_z_chunks(sf_solver* s, int chunks);
 
+/* Launch tuning of the x pass (no counterpart in the reference): lane groups
+ * (one transform at a time each) per block, 1..32 (0: enough for one slab's
+ * inverse transforms in one round). More groups keep more warps resident;
+ * groups without a task in a round idle through it. Results do not depend
+ * on it. */
+int sf_set_xpass_groups(sf_solver* s, int groups);
+
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 

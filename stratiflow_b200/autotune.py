@@ -8,6 +8,8 @@ kernels' launch shapes, which change no result (or only its rounding):
 
   xslabs    z-slabs one x-pass block walks through (sf_set_xpass_slabs;
             0 = the launcher's own choice)
+  xgroups   lane groups per x-pass block (sf_set_xpass_groups; 0 = enough
+            for one slab's inverse transforms in one round)
   xy_bands  level bands of the 3D x-y pass whose y transforms run beside the
             neighbouring bands' x passes (sf_set_xy_bands; 3D only)
   z_chunks  z-chunks per block of the z solves (sf_set_z_chunks; 0 = the
@@ -27,8 +29,8 @@ import os
 import time
 from typing import Callable, Dict, List, Tuple
 
-DEFAULTS = {"xslabs": 0, "xy_bands": 1, "z_chunks": 0}
-ORDER = ("xy_bands", "xslabs", "z_chunks")
+DEFAULTS = {"xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0}
+ORDER = ("xy_bands", "xslabs", "xgroups", "z_chunks")
 MARGIN = 0.02   # a candidate must be 2% faster to replace the current value
 
 _memory: Dict[str, dict] = {}
@@ -40,6 +42,7 @@ def space(N2: int, N3: int) -> Dict[str, List[int]]:
         "xy_bands": [1, 2, 3, 4, 6, 8] if N2 > 1 else [DEFAULTS["xy_bands"]],
         "xslabs": [0, 1, 2, 3, 4, 6, 8],
         "z_chunks": [0] + [c for c in (8, 16) if N3 >= 2 * c],
+        "xgroups": [0, 8, 16],
     }
 
 
@@ -126,6 +129,7 @@ def apply(solver, settings: dict) -> None:
     if solver.N2 > 1:
         solver.set_xy_bands(int(settings["xy_bands"]))
     solver.set_z_chunks(int(settings["z_chunks"]))
+    solver.set_xpass_groups(int(settings.get("xgroups", 0)))
 
 
 def device_name(solver) -> str:

@@ -82,6 +82,7 @@ struct StageArgs {
   // xcols = 0: all), for the banded 3D x-y pass
   int lvl0, nlvl, xcol0, xcols;
   int zchunks;      // z chunks per block of the z solves (8 or 16; 0: chosen by the launcher)
+  int xgroups;      // lane groups per x-pass block (0: chosen by the launcher)
 };
 
 // side streams and events of the banded 3D x-y pass: the inverse y

@@ -1285,7 +1285,7 @@ static XShape xpass_shape(const StageArgs& a, int nruns) {
   // threads: enough lane groups for all phase-A transforms of a slab (one
   // round), at least two warps, at most kXMaxThreads
   auto threads = [&](int S) {
-    int groups = 2 * (S + 2);
+    int groups = a.xgroups > 0 ? a.xgroups : 2 * (S + 2);
     int t = ((groups * G + 31) / 32) * 32;
     return t < 64 ? 64 : (t > kXMaxThreads ? kXMaxThreads : t);
   };

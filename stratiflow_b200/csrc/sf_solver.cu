@@ -57,6 +57,7 @@ struct sf_solver {
   XYAux xy{};                    // side streams of the banded 3D x-y pass
   int xy_bands = 1;              // level bands of the 3D x-y pass (sf_set_xy_bands)
   int zchunks = 0;               // z chunks per z-solve block (sf_set_z_chunks)
+  int xgroups = 0;               // lane groups per x-pass block (sf_set_xpass_groups)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -219,6 +220,7 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.run_offset = 0;
   a.xslabs = s->xslabs;
   a.zchunks = s->zchunks;
+  a.xgroups = s->xgroups;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -813,6 +815,15 @@ int sf_cfl(sf_solver* s, int run, double* cfl) {
   const Geo& g = s->g;
   const double d1 = s->L1 / g.N1, d2 = s->L2 / g.N2, d3 = s->zN[g.N3 / 2 + 1] - s->zN[g.N3 / 2];
   *cfl = (m[0] / d1 + (g.dim3 ? m[1] / d2 : 0.0) + m[2] / d3) * s->dt;
+  return SF_OK;
+}
+
+int sf_set_xpass_groups(sf_solver* s, int groups) {
+  if (!s || groups < 0 || groups > 32) return fail(SF_EINVAL, "groups must be in [0, 32]");
+  if (groups != s->xgroups) {
+    s->xgroups = groups;
+    drop_graphs(s);
+  }
   return SF_OK;
 }
 
