@@ -106,7 +106,7 @@ def store(key: str, settings: dict, path: str | None = None) -> None:
     d[key] = dict(settings)
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"   # processes sharing the cache (ranks) write their own
         with open(tmp, "w") as f:
             json.dump(d, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
