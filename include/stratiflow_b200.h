@@ -199,6 +199,15 @@ int sf_set_z_chunks(sf_solver* s, int chunks);
  * on it. */
 int sf_set_xpass_groups(sf_solver* s, int groups);
 
+/* Launch tuning of the 3D nonlinear x pass (no counterpart in the reference):
+ * kind 1 (the default) runs it as lane groups that each own a y row and
+ * march up a range of levels, transforming two fields or products per packed
+ * FP32 instruction; kind 0 as blocks over slabs of levels (the kernel that
+ * every other x pass uses). The results agree to rounding (the z stencils'
+ * terms are summed in another order). Grids with N1 other than 64, 128 or 256
+ * always take kind 0. */
+int sf_set_xpass_kernel(sf_solver* s, int kind);
+
 /* IMEXRK::KE / PE (IMEXRK.h:395-411) of one run, accumulated in FP64 */
 int sf_energy(sf_solver* s, int run, double* ke, double* pe);
 

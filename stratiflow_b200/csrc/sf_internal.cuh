@@ -83,6 +83,7 @@ struct StageArgs {
   int lvl0, nlvl, xcol0, xcols;
   int zchunks;      // z chunks per block of the z solves (8 or 16; 0: chosen by the launcher)
   int xgroups;      // lane groups per x-pass block (0: chosen by the launcher)
+  int xkernel;      // 3D nonlinear x pass: 1 level-marching lane groups (k_xmarch), 0 slab blocks (k_xpass)
 };
 
 // side streams and events of the banded 3D x-y pass: the inverse y
@@ -106,6 +107,11 @@ constexpr int kEnsThreads = 256;
 
 // launchers (sf_kernels.cu); each returns the number of kernels launched
 int prepare_kernels();
+// the 3D nonlinear x pass as level-marching lane groups (sf_xmarch.cu): levels
+// t_lo .. t_hi - 1 of every run and y row
+bool xmarch_supported(const StageArgs& a);
+int launch_xmarch(const StageArgs& a, int t_lo, int t_hi, cudaStream_t st);
+int prepare_xmarch_kernels();
 // one stage; if ev != nullptr, ev[i] is recorded after the i-th kernel
 int launch_stage(const StageArgs& a, cudaStream_t st, cudaEvent_t* ev = nullptr, const XYAux* aux = nullptr);
 int stage_kernel_count(const Geo& g);

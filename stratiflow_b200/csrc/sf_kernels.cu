@@ -1369,6 +1369,13 @@ static int launch_xpass(const StageArgs& a, cudaStream_t st) {
   }
   StageArgs b = a;
   b.run_offset = 0;
+  if (a.xkernel == 1 && xmarch_supported(a)) {
+    // the same level columns as the slab kernel's launch would cover
+    const int lv = xpass_column_levels(a, false, a.g.nrun);
+    const int ncol = (int)cdiv(a.g.N3, lv);
+    const int c1 = a.xcols > 0 ? a.xcol0 + a.xcols : ncol;
+    return launch_xmarch(b, a.xcol0 * lv, std::min(a.g.N3, c1 * lv), st);
+  }
   launch_xpass_runs(b, a.linear != 0, a.g.nrun, st);
   return 1;
 }
@@ -1422,6 +1429,7 @@ int prepare_kernels() {
   ATTR(k_z_proj_chunked<8>) ATTR(k_z_proj_chunked<16>)
   ATTR((k_z_step<8, false>)) ATTR((k_z_step<8, true>)) ATTR((k_z_step<16, false>)) ATTR((k_z_step<16, true>))
 #undef ATTR
+  if (e == cudaSuccess && prepare_xmarch_kernels() != 0) return -1;
   return e == cudaSuccess ? 0 : -1;
 }
 

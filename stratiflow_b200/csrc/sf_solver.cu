@@ -58,6 +58,7 @@ struct sf_solver {
   int xy_bands = 1;              // level bands of the 3D x-y pass (sf_set_xy_bands)
   int zchunks = 0;               // z chunks per z-solve block (sf_set_z_chunks)
   int xgroups = 0;               // lane groups per x-pass block (sf_set_xpass_groups)
+  int xkernel = 1;               // 3D nonlinear x pass: 1 level-marching, 0 slab blocks (sf_set_xpass_kernel)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -221,6 +222,7 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.xslabs = s->xslabs;
   a.zchunks = s->zchunks;
   a.xgroups = s->xgroups;
+  a.xkernel = s->xkernel;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -822,6 +824,15 @@ int sf_set_xpass_groups(sf_solver* s, int groups) {
   if (!s || groups < 0 || groups > 32) return fail(SF_EINVAL, "groups must be in [0, 32]");
   if (groups != s->xgroups) {
     s->xgroups = groups;
+    drop_graphs(s);
+  }
+  return SF_OK;
+}
+
+int sf_set_xpass_kernel(sf_solver* s, int kind) {
+  if (!s || (kind != 0 && kind != 1)) return fail(SF_EINVAL, "kind must be 0 or 1");
+  if (kind != s->xkernel) {
+    s->xkernel = kind;
     drop_graphs(s);
   }
   return SF_OK;
