@@ -23,8 +23,12 @@ struct c2x {
 
 __device__ __forceinline__ float2 pk2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
-// a - b as one fused multiply-add, b * (-1) + a (exact, one rounding)
-__device__ __forceinline__ float2 psub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+// a - b (packed subtraction, sub.rn.f32x2)
+__device__ __forceinline__ float2 psub(float2 a, float2 b) {
+  unsigned long long x = *reinterpret_cast<const unsigned long long*>(&a), y = *reinterpret_cast<const unsigned long long*>(&b), d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(x), "l"(y));
+  return *reinterpret_cast<float2*>(&d);
+}
 __device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 
@@ -92,38 +96,39 @@ __device__ __forceinline__ void fill_tw2(float4* tw4, float2* tw2, const float2*
   }
 }
 
-// a * w (or a * conj(w) for the inverse) with w's table entries loaded and
-// used in one block of instructions, so that the compiler does not load a
-// transform's fifteen twiddles ahead into registers (six per twiddle)
+// a * w (or a * conj(w) for the inverse), w from its table entry (wr, wr, wi,
+// wi): one 128-bit shared load and five packed operations. The load and the
+// arithmetic are one block of instructions, so that the compiler does not load
+// a transform's twiddles ahead into registers (four per twiddle).
 template <bool INV>
-__device__ __forceinline__ void tw2_apply(c2x& a, const float4* t4, const float2* t2) {
+__device__ __forceinline__ void tw2_apply(c2x& a, const float4* t4, const float2* /*t2*/) {
   unsigned long long re = *reinterpret_cast<const unsigned long long*>(&a.re);
   unsigned long long im = *reinterpret_cast<const unsigned long long*>(&a.im);
-  const unsigned s4 = (unsigned)__cvta_generic_to_shared(t4), s2 = (unsigned)__cvta_generic_to_shared(t2);
+  const unsigned s4 = (unsigned)__cvta_generic_to_shared(t4);
   if (INV)   // re' = re wr + im wi, im' = im wr - re wi
     asm volatile(
-        "{\n\t.reg .b64 wr, wi, nwi, p, q;\n\t"
+        "{\n\t.reg .b64 wr, wi, p, q;\n\t"
         "ld.shared.v2.b64 {wr, wi}, [%2];\n\t"
-        "ld.shared.b64 nwi, [%3];\n\t"
-        "mul.rn.f32x2 p, %0, wr;\n\t"
+        "mul.rn.f32x2 p, %1, wi;\n\t"
         "mul.rn.f32x2 q, %1, wr;\n\t"
-        "fma.rn.f32x2 p, %1, wi, p;\n\t"
-        "fma.rn.f32x2 %1, %0, nwi, q;\n\t"
+        "fma.rn.f32x2 p, %0, wr, p;\n\t"
+        "mul.rn.f32x2 %1, %0, wi;\n\t"
+        "sub.rn.f32x2 %1, q, %1;\n\t"
         "mov.b64 %0, p;\n\t}"
         : "+l"(re), "+l"(im)
-        : "r"(s4), "r"(s2));
+        : "r"(s4));
   else       // re' = re wr - im wi, im' = re wi + im wr
     asm volatile(
-        "{\n\t.reg .b64 wr, wi, nwi, p, q;\n\t"
+        "{\n\t.reg .b64 wr, wi, p, q;\n\t"
         "ld.shared.v2.b64 {wr, wi}, [%2];\n\t"
-        "ld.shared.b64 nwi, [%3];\n\t"
-        "mul.rn.f32x2 p, %0, wr;\n\t"
-        "mul.rn.f32x2 q, %1, wr;\n\t"
-        "fma.rn.f32x2 p, %1, nwi, p;\n\t"
-        "fma.rn.f32x2 %1, %0, wi, q;\n\t"
+        "mul.rn.f32x2 p, %1, wi;\n\t"
+        "mul.rn.f32x2 q, %0, wr;\n\t"
+        "sub.rn.f32x2 p, q, p;\n\t"
+        "mul.rn.f32x2 q, %0, wi;\n\t"
+        "fma.rn.f32x2 %1, %1, wr, q;\n\t"
         "mov.b64 %0, p;\n\t}"
         : "+l"(re), "+l"(im)
-        : "r"(s4), "r"(s2));
+        : "r"(s4));
   a.re = *reinterpret_cast<float2*>(&re);
   a.im = *reinterpret_cast<float2*>(&im);
 }
@@ -161,6 +166,63 @@ __device__ __forceinline__ void reg_fft2(c2x (&x)[FFTShape<N>::E], float4* buf, 
     dft2<G, INV>(y[h]);
 #pragma unroll
     for (int k2 = 0; k2 < G; k2++) x[h * G + k2] = y[h][k2];
+  }
+}
+
+// The packed transform pair of N = 256 points over a whole warp (32 lanes,
+// 8 points each) in three stages: on entry lane l holds in[l + 32 e] in slot e
+// (e < 8); an 8-point DFT over e and W_256^{l k1}; a transpose so that lane
+// (k1 = l % 8, l0 = l / 8) holds column k1 at l0 + 4 l1 (l1 < 8); an 8-point
+// DFT over l1 and W_32^{l0 m} (= W_256^{8 l0 m}, the same table); a transpose
+// so that lane l holds the values l0 = 0..3 of (k1 = l % 8, m = l / 8 + 4 h),
+// h = 0, 1; two 4-point DFTs over l0. On exit slot h*4 + q holds
+// out[l + 32 h + 64 q], i.e. out[l + 32 j] with j = h + 2q. tw4 / tw2 are the
+// table of fill_tw2_256w: [k1][l], W_256^{l k1}, k1 < 8, l < 32. buf holds
+// 8 x 33 float4 (padded columns: every access conflict-free).
+__device__ __forceinline__ void fill_tw2_256w(float4* tw4, float2* tw2, const float2* __restrict__ tw, int tid,
+                                              int nthr) {
+  for (int i = tid; i < 8 * 32; i += nthr) {
+    const int k1 = i / 32, l = i - k1 * 32;
+    const float2 w = tw[(l * k1) * (kMaxN / 256)];
+    tw4[i] = make_float4(w.x, w.x, w.y, w.y);
+    tw2[i] = make_float2(-w.y, -w.y);
+  }
+}
+
+__device__ __forceinline__ float4 c2x_to4(const c2x& v) { return make_float4(v.re.x, v.re.y, v.im.x, v.im.y); }
+__device__ __forceinline__ c2x c2x_of4(const float4 v) { return c2x{make_float2(v.x, v.y), make_float2(v.z, v.w)}; }
+
+template <bool INV>
+__device__ __forceinline__ void reg_fft2_256w(c2x (&x)[8], float4* buf, const float4* __restrict__ tw4,
+                                              const float2* __restrict__ tw2, int l) {
+  dft2<8, INV>(x);
+#pragma unroll
+  for (int k1 = 1; k1 < 8; k1++) tw2_apply<INV>(x[k1], tw4 + k1 * 32 + l, tw2 + k1 * 32 + l);
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < 8; k1++) buf[k1 * 33 + l] = c2x_to4(x[k1]);   // element (row l, column k1)
+  __syncwarp();
+  const int k1 = l & 7, l0 = l >> 3;
+#pragma unroll
+  for (int l1 = 0; l1 < 8; l1++) x[l1] = c2x_of4(buf[k1 * 33 + l0 + 4 * l1]);
+  __syncwarp();
+  dft2<8, INV>(x);
+#pragma unroll
+  for (int m = 1; m < 8; m++) tw2_apply<INV>(x[m], tw4 + m * 32 + 8 * l0, tw2 + m * 32 + 8 * l0);
+#pragma unroll
+  for (int m = 0; m < 8; m++) buf[m * 33 + l] = c2x_to4(x[m]);         // element (lane l, m)
+  __syncwarp();
+  c2x y[2][4];
+#pragma unroll
+  for (int h = 0; h < 2; h++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) y[h][q] = c2x_of4(buf[((l >> 3) + 4 * h) * 33 + (l & 7) + 8 * q]);
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    dft2<4, INV>(y[h]);
+#pragma unroll
+    for (int q = 0; q < 4; q++) x[h * 4 + q] = y[h][q];
   }
 }
 

@@ -3,8 +3,8 @@
 // x part with 1/(N1 N2) and the 2/3 truncation, then the x derivatives and the
 // z stencils that follow each product).
 //
-// One lane group (G lanes, FFTShape<N1>) owns one y row and walks up a range
-// of z levels. At level t it inverse-transforms the four fields of level t
+// One lane group (XMT<N1>::G lanes: the whole warp at N1 = 256, else
+// FFTShape<N1>::G lanes) owns one y row and walks up a range of z levels. At level t it inverse-transforms the four fields of level t
 // (u1 + i u3 and b + i u2, packed as one two-transform pair, sf_fft2.cuh),
 // keeps them in registers and the fields of level t-1 in its own shared
 // memory, forms the eleven products of level t (with P4 of level t-1, the one
@@ -27,44 +27,71 @@
 
 namespace sf {
 
-constexpr int kXMWarps = 6;   // warps per block; one block per SM at N1 = 256
+// Lane layout of the march for one grid width N1: G lanes per y row, E x
+// points per lane (x = l + G e), W rows per warp, the output slots that hold
+// the kept modes, and the packed transform pair.
+template <int N1>
+struct XMT {   // N1 = 64, 128: two-stage transforms over FFTShape<N1>::G lanes
+  static constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, H = E / G, K1 = N1 / 3;
+  static constexpr int W = 32 / G;                  // rows per warp
+  static constexpr int WARPS = 6;                   // warps per block
+  static constexpr int NK2 = (K1 - 1) / E + 1;
+  static constexpr int NKS = H * NK2;               // output slots holding a kept mode for some lane
+  static constexpr int TB = fft2_buf_elems<N1>();   // float4 per transpose buffer
+  static constexpr int TWE = E * G;                 // twiddle table entries
+  // output slot of the i-th kept candidate; slot h*G + k2 holds mode l + h*G + E*k2
+  __host__ __device__ static constexpr int kslot(int i) { return (i / NK2) * G + i % NK2; }
+  __device__ static int kmode(int l, int i) { return l + (kslot(i) / G) * G + E * (kslot(i) % G); }
+  // x position index e (x = l + G e) of inverse output slot s
+  __host__ __device__ static constexpr int pos(int s) { return s / G + H * (s % G); }
+  // slot holding mode N1 - k at lane G - l (l >= 1) or at lane 0 (l = 0)
+  __host__ __device__ static constexpr int partner(int i, bool lane0) {
+    const int s = kslot(i), h = s / G, k2 = s % G;
+    const int q = lane0 ? (E - h - H * k2) % E : E - 1 - h - H * k2;
+    return (q % H) * G + q / H;
+  }
+  __device__ static void fill(float4* tw4, float2* tw2, const float2* tw, int tid, int nthr) {
+    fill_tw2<N1>(tw4, tw2, tw, tid, nthr);
+  }
+  template <bool INV>
+  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l) {
+    reg_fft2<N1, INV>(x, buf, tw4, tw2, l);
+  }
+};
+template <>
+struct XMT<256> {   // a whole warp per row: three stages, 8 x 8 x 4 (reg_fft2_256w)
+  static constexpr int G = 32, E = 8, K1 = 85, W = 1, WARPS = 12;
+  static constexpr int NKS = 3;                     // modes l, l + 32, l + 64
+  static constexpr int TB = 8 * 33, TWE = 8 * 32;
+  // slot of out[l + 32 j]: j = h + 2 q in slot h*4 + q
+  __host__ __device__ static constexpr int jslot(int j) { return (j % 2) * 4 + j / 2; }
+  __host__ __device__ static constexpr int kslot(int i) { return jslot(i); }
+  __device__ static int kmode(int l, int i) { return l + 32 * i; }
+  __host__ __device__ static constexpr int pos(int s) { return s / 4 + 2 * (s % 4); }
+  __host__ __device__ static constexpr int partner(int i, bool lane0) { return jslot(lane0 ? (8 - i) % 8 : 7 - i); }
+  __device__ static void fill(float4* tw4, float2* tw2, const float2* tw, int tid, int nthr) {
+    fill_tw2_256w(tw4, tw2, tw, tid, nthr);
+  }
+  template <bool INV>
+  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l) {
+    reg_fft2_256w<INV>(x, buf, tw4, tw2, l);
+  }
+};
 
 template <int N1>
-struct XMShape {
-  static constexpr int G = FFTShape<N1>::G, E = FFTShape<N1>::E, H = E / G, K1 = N1 / 3;
-  static constexpr int W = 32 / G;                  // groups (y rows) per warp
-  static constexpr int NK2 = (K1 - 1) / E + 1;      // k2 values whose slots hold kept modes
-  static constexpr int NKS = H * NK2;               // output slots that hold a kept mode for some lane
-  static constexpr int TB = fft2_buf_elems<N1>();   // float4 of one transpose buffer
-  // shared memory of one group: two levels of nodal values (float4 per x
+struct XMShape : XMT<N1> {
+  using T = XMT<N1>;
+  // shared memory of one row: two levels of nodal values (float4 per x
   // point, a ring: this level and the one below), the transpose buffer, the
   // carried combinations ((c1, cB), (c2, c3) per kept slot and lane) and the
   // staged input rows of the next level (4 x K1)
-  static constexpr size_t group_bytes = sizeof(float4) * (size_t)(2 * N1 + TB + 2 * NKS * G) + sizeof(float2) * 4 * K1;
-  static constexpr size_t table_bytes = (sizeof(float4) + sizeof(float2)) * (size_t)E * G;
-  static constexpr size_t smem_bytes = table_bytes + (size_t)kXMWarps * W * group_bytes;
+  static constexpr size_t group_bytes =
+      sizeof(float4) * (size_t)(2 * N1 + T::TB + 2 * T::NKS * T::G) + sizeof(float2) * 4 * T::K1;
+  static constexpr size_t table_bytes = (sizeof(float4) + sizeof(float2)) * (size_t)T::TWE;
+  static constexpr size_t smem_bytes = table_bytes + (size_t)T::WARPS * T::W * group_bytes;
   static_assert(group_bytes % 16 == 0 && table_bytes % 16 == 0, "16-byte aligned regions");
+  static_assert(smem_bytes <= 227 * 1024, "one block fits an SM");
 };
-
-// output slot of the i-th kept-mode candidate (slot h*G + k2 holds mode l + h*G + E*k2)
-template <int N1>
-__host__ __device__ constexpr int xm_kslot(int i) {
-  return (i / XMShape<N1>::NK2) * XMShape<N1>::G + i % XMShape<N1>::NK2;
-}
-// x position index e (x = l + G e) of inverse-transform output slot s
-template <int N1>
-__host__ __device__ constexpr int xm_pos(int s) {
-  return s / XMShape<N1>::G + XMShape<N1>::H * (s % XMShape<N1>::G);
-}
-// slot holding mode N1 - k at lane G - l (l >= 1) and at lane 0 (l = 0), for
-// the mode k of slot s at lane l
-template <int N1>
-__host__ __device__ constexpr int xm_partner(int s, bool lane0) {
-  constexpr int G = XMShape<N1>::G, E = XMShape<N1>::E, H = XMShape<N1>::H;
-  const int h = s / G, k2 = s % G;
-  const int q = lane0 ? (E - h - H * k2) % E : E - 1 - h - H * k2;
-  return (q % H) * G + q / H;
-}
 
 __device__ __forceinline__ void xm_cp8(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
@@ -77,22 +104,23 @@ __device__ __forceinline__ float4 c2x_f4(const c2x& v) { return make_float4(v.re
 // levels t_lo .. t_hi - 1 of every (run, y row) of the launch; the units
 // (run, block of W rows, level) are split evenly over the launch's warps
 template <int N1>
-__global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_lo, int t_hi) {
+__global__ void __launch_bounds__(XMT<N1>::WARPS * 32, 1) k_xmarch(StageArgs a, int t_lo, int t_hi) {
   using X = XMShape<N1>;
-  constexpr int G = X::G, E = X::E, K1 = X::K1, W = X::W, NKS = X::NKS;
+  using T = XMT<N1>;
+  constexpr int G = T::G, E = T::E, K1 = T::K1, W = T::W, NKS = T::NKS, kXMWarps = T::WARPS;
   const Geo g = a.g;
   const int N3 = g.N3, N2 = g.N2;
   extern __shared__ __align__(16) unsigned char xsm[];
   float4* tw4 = reinterpret_cast<float4*>(xsm);
-  float2* tw2 = reinterpret_cast<float2*>(xsm + sizeof(float4) * E * G);
-  fill_tw2<N1>(tw4, tw2, a.tw, threadIdx.x, blockDim.x);
+  float2* tw2 = reinterpret_cast<float2*>(xsm + sizeof(float4) * T::TWE);
+  T::fill(tw4, tw2, a.tw, threadIdx.x, blockDim.x);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int gw = lane / G, l = lane - gw * G;
   __builtin_assume(l >= 0 && l < G);
   unsigned char* gb = xsm + X::table_bytes + (size_t)(warp * W + gw) * X::group_bytes;
   float4* ring = reinterpret_cast<float4*>(gb);     // [2 levels][E slots][G lanes]: u1, b, u3, u2
   float4* tbuf = ring + 2 * N1;                     // transpose buffer
-  float4* cbuf = tbuf + X::TB;                      // [2][NKS][G]: (c1, cB), (c2, c3) awaiting their z terms
+  float4* cbuf = tbuf + T::TB;                      // [2][NKS][G]: (c1, cB), (c2, c3) awaiting their z terms
   float2* stg = reinterpret_cast<float2*>(cbuf + 2 * NKS * G);   // [4][K1]: u1, u2, u3, b of the next level
   __syncthreads();
 
@@ -140,7 +168,7 @@ __global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_
       }
     };
     // this lane's kept mode in kept slot i
-    auto kk = [&](int i) { return l + (xm_kslot<N1>(i) / G) * G + E * (xm_kslot<N1>(i) % G); };
+    auto kk = [&](int i) { return T::kmode(l, i); };
     // c1, cB and c2, c3 of the last level, awaiting their z terms, per kept slot
     auto Ca = [&](int i) -> float4& { return cbuf[i * G + l]; };
     auto Cb = [&](int i) -> float4& { return cbuf[(NKS + i) * G + l]; };
@@ -187,7 +215,7 @@ __global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_
       float4* curl = ring + (size_t)(t & 1) * N1;
       const float4* prev = ring + (size_t)((t - 1) & 1) * N1;
       if (lv) {
-        reg_fft2<N1, true>(x, tbuf, tw4, tw2, l);
+        T::template fft<true>(x, tbuf, tw4, tw2, l);
 #pragma unroll
         for (int s = 0; s < E; s++) curl[s * G + l] = c2x_f4(x[s]);
         tok = __float_as_int(x[0].re.x) & rz;
@@ -228,7 +256,7 @@ __global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_
             const float qb = (hb * Bv + hb * pv.y) * w3;
             const float q2 = (hb * U2 + hb * pv.w) * w3;
             const float d = 0.5f * pv.z + 0.5f * topm * U3;
-            z[xm_pos<N1>(s)] = c2x{make_float2(q1, q2), make_float2(qb, lm * (d * d))};
+            z[T::pos(s)] = c2x{make_float2(q1, q2), make_float2(qb, lm * (d * d))};
           }
         } else if (b == 1) {
 #pragma unroll
@@ -236,7 +264,7 @@ __global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_
             const float4 cv = curl[s * G + l + tok];
             const float U1 = cv.x, Bv = cv.y, U2 = cv.w;
             const float u1t = U1 + ub;
-            z[xm_pos<N1>(s)] = c2x{make_float2(U1 * (U1 + 2.f * ub), u1t * U2), make_float2(u1t * Bv, U2 * U2)};
+            z[T::pos(s)] = c2x{make_float2(U1 * (U1 + 2.f * ub), u1t * U2), make_float2(u1t * Bv, U2 * U2)};
           }
         } else {
 #pragma unroll
@@ -246,24 +274,24 @@ __global__ void __launch_bounds__(kXMWarps * 32, 1) k_xmarch(StageArgs a, int t_
             const float w3 = lof * U3;
             const float p3 = (tdi * U1 + tlo * pv.x + (tlo * ubm + tdi * ub)) * w3;
             const float p3y = (tdi * U2 + tlo * pv.w) * w3;
-            z[xm_pos<N1>(s)] = c2x{make_float2(p3, U2 * Bv), make_float2(p3y, 0.f)};
+            z[T::pos(s)] = c2x{make_float2(p3, U2 * Bv), make_float2(p3y, 0.f)};
           }
         }
-        reg_fft2<N1, false>(z, tbuf, tw4, tw2, l);
+        T::template fft<false>(z, tbuf, tw4, tw2, l);
         // split each transform of the pair into its two real products at
         // the kept modes: (Z_k + conj Z_{N-k}) / 2 and (Z_k - conj Z_{N-k}) / (2i),
         // times 1/(N1 N2)
 #pragma unroll
         for (int i = 0; i < NKS; i++) {
-          const int s = xm_kslot<N1>(i);
+          const int s = T::kslot(i);
           const c2x zs = z[s];
-          const c2x po = z[xm_partner<N1>(s, false)];
+          const c2x po = z[T::partner(i, false)];
           c2x p;
           p.re.x = __shfl_sync(0xffffffffu, po.re.x, partner_lane);
           p.re.y = __shfl_sync(0xffffffffu, po.re.y, partner_lane);
           p.im.x = __shfl_sync(0xffffffffu, po.im.x, partner_lane);
           p.im.y = __shfl_sync(0xffffffffu, po.im.y, partner_lane);
-          if (l == 0) p = z[xm_partner<N1>(s, true)];
+          if (l == 0) p = z[T::partner(i, true)];
           if (kk(i) >= K1) continue;
           const float2 SR = pmul(padd(zs.re, p.re), SC), DI = pmul(psub(zs.im, p.im), SC);
           const float2 SI = pmul(padd(zs.im, p.im), SC), DR = pmul(psub(p.re, zs.re), SC);
@@ -309,10 +337,10 @@ static int xmarch_launch(const StageArgs& a, int t_lo, int t_hi, cudaStream_t st
     int dev = 0, nsm = 0, bps = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_xmarch<N1>, kXMWarps * 32, X::smem_bytes);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_xmarch<N1>, X::WARPS * 32, X::smem_bytes);
     blocks = std::max(1, bps) * std::max(1, nsm);
   }
-  k_xmarch<N1><<<blocks, kXMWarps * 32, X::smem_bytes, st>>>(a, t_lo, t_hi);
+  k_xmarch<N1><<<blocks, X::WARPS * 32, X::smem_bytes, st>>>(a, t_lo, t_hi);
   return 1;
 }
 
@@ -321,7 +349,7 @@ bool xmarch_supported(const StageArgs& a) {
   if (!g.dim3 || a.linear || a.tlm || a.adjoint) return false;
   const int N1 = g.N1;
   if (N1 != 64 && N1 != 128 && N1 != 256) return false;
-  const int W = 32 / (N1 == 256 ? 16 : 8);
+  const int W = N1 == 256 ? XMT<256>::W : 4;
   return g.N2 % W == 0;
 }
 
