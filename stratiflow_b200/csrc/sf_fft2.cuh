@@ -192,12 +192,20 @@ __device__ __forceinline__ void fill_tw2_256w(float4* tw4, float2* tw2, const fl
 __device__ __forceinline__ float4 c2x_to4(const c2x& v) { return make_float4(v.re.x, v.re.y, v.im.x, v.im.y); }
 __device__ __forceinline__ c2x c2x_of4(const float4 v) { return c2x{make_float2(v.x, v.y), make_float2(v.z, v.w)}; }
 
+// a * w (a * conj(w) for the inverse) with WR = (wr, wr), WI = (wi, wi) in registers
+template <bool INV>
+__device__ __forceinline__ c2x tw2_mul_reg(const c2x a, const float4 w) {
+  const float2 WR = make_float2(w.x, w.y), WI = make_float2(w.z, w.w);
+  if (INV) return c2x{pfma(a.re, WR, pmul(a.im, WI)), psub(pmul(a.im, WR), pmul(a.re, WI))};
+  return c2x{psub(pmul(a.re, WR), pmul(a.im, WI)), pfma(a.im, WR, pmul(a.re, WI))};
+}
+
 template <bool INV>
 __device__ __forceinline__ void reg_fft2_256w(c2x (&x)[8], float4* buf, const float4* __restrict__ tw4,
-                                              const float2* __restrict__ tw2, int l) {
+                                              const float2* __restrict__ tw2, int l, const float4 (&w1)[8]) {
   dft2<8, INV>(x);
 #pragma unroll
-  for (int k1 = 1; k1 < 8; k1++) tw2_apply<INV>(x[k1], tw4 + k1 * 32 + l, tw2 + k1 * 32 + l);
+  for (int k1 = 1; k1 < 8; k1++) x[k1] = tw2_mul_reg<INV>(x[k1], w1[k1]);
   __syncwarp();
 #pragma unroll
   for (int k1 = 0; k1 < 8; k1++) buf[k1 * 33 + l] = c2x_to4(x[k1]);   // element (row l, column k1)

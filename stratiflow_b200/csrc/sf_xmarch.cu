@@ -54,7 +54,8 @@ struct XMT {   // N1 = 64, 128: two-stage transforms over FFTShape<N1>::G lanes
     fill_tw2<N1>(tw4, tw2, tw, tid, nthr);
   }
   template <bool INV>
-  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l) {
+  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l,
+                             const float4 (&)[8]) {
     reg_fft2<N1, INV>(x, buf, tw4, tw2, l);
   }
 };
@@ -73,8 +74,9 @@ struct XMT<256> {   // a whole warp per row: three stages, 8 x 8 x 4 (reg_fft2_2
     fill_tw2_256w(tw4, tw2, tw, tid, nthr);
   }
   template <bool INV>
-  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l) {
-    reg_fft2_256w<INV>(x, buf, tw4, tw2, l);
+  __device__ static void fft(c2x (&x)[E], float4* buf, const float4* tw4, const float2* tw2, int l,
+                             const float4 (&w1)[8]) {
+    reg_fft2_256w<INV>(x, buf, tw4, tw2, l, w1);
   }
 };
 
@@ -125,6 +127,10 @@ __global__ void __launch_bounds__(XMT<N1>::WARPS * 32, 1) k_xmarch(StageArgs a, 
   __syncthreads();
 
   const int partner_lane = (lane & ~(G - 1)) | ((G - l) & (G - 1));
+  // the first-stage twiddles of the whole-warp transform, held in registers
+  float4 w1[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) w1[k] = (N1 == 256) ? tw4[(k * 32 + l) % T::TWE] : make_float4(0.f, 0.f, 0.f, 0.f);
   // zero, but not known to the compiler: a batch's shared-memory reads take
   // (bits of the last batch's result) & rz as an offset, a true dependency
   // that keeps the compiler from starting one batch's products and
@@ -215,7 +221,7 @@ __global__ void __launch_bounds__(XMT<N1>::WARPS * 32, 1) k_xmarch(StageArgs a, 
       float4* curl = ring + (size_t)(t & 1) * N1;
       const float4* prev = ring + (size_t)((t - 1) & 1) * N1;
       if (lv) {
-        T::template fft<true>(x, tbuf, tw4, tw2, l);
+        T::template fft<true>(x, tbuf, tw4, tw2, l, w1);
 #pragma unroll
         for (int s = 0; s < E; s++) curl[s * G + l] = c2x_f4(x[s]);
         tok = __float_as_int(x[0].re.x) & rz;
@@ -277,7 +283,7 @@ __global__ void __launch_bounds__(XMT<N1>::WARPS * 32, 1) k_xmarch(StageArgs a, 
             z[T::pos(s)] = c2x{make_float2(p3, U2 * Bv), make_float2(p3y, 0.f)};
           }
         }
-        T::template fft<false>(z, tbuf, tw4, tw2, l);
+        T::template fft<false>(z, tbuf, tw4, tw2, l, w1);
         // split each transform of the pair into its two real products at
         // the kept modes: (Z_k + conj Z_{N-k}) / 2 and (Z_k - conj Z_{N-k}) / (2i),
         // times 1/(N1 N2)
