@@ -198,7 +198,7 @@ def kernel_bytes(s, name):
     nf = 4 if s.dim3 else 3
     if name == "k_ifft_y":
         return 4 * S + 4 * M
-    if name == "k_xpass":
+    if name in ("k_xpass", "k_xmarch"):
         return (4 * M + 8 * M) if s.dim3 else (3 * S + 3 * S)
     if name == "k_fft_y":
         return 8 * M + 4 * S

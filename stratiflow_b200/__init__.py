@@ -467,6 +467,8 @@ class IMEXRK:
         buf = C.create_string_buffer(4096)
         _check(L.sf_profile_names(self._h, buf, 4096))
         names = buf.value.decode().split(",")
+        if linear:   # TimeStepLinear's x pass is the slab kernel
+            names = ["k_xpass" if nm == "k_xmarch" else nm for nm in names]
         return [(f"s{i // (n.value // 3)}:{names[i]}", ms[i]) for i in range(n.value)]
 
     def launch_count(self):

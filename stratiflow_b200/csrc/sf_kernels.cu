@@ -20,6 +20,7 @@
 #include <type_traits>
 #include "sf_internal.cuh"
 #include "sf_fft.cuh"
+#include "sf_fft2.cuh"
 
 namespace sf {
 
@@ -65,12 +66,60 @@ __global__ void __launch_bounds__(kYThreads, 8) k_ifft_y(StageArgs a) {
   }
 }
 
+// The same for fields (2p, 2p+1) of every run at once (blockIdx.z = 2 run +
+// p): each lane group transforms its column of both fields as one packed pair
+// of transforms (sf_fft2.cuh), half the FP32 instructions of two transforms.
+template <int N2>
+__global__ void __launch_bounds__(kYThreads) k_ifft_y2(StageArgs a) {
+  constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E;
+  const Geo g = a.g;
+  __shared__ float4 fbuf4[(kYThreads / G) * fft2_buf_elems<N2>()];
+  __shared__ float4 tw4[E * G];
+  __shared__ float2 tw2[E * G];
+  fill_tw2<N2>(tw4, tw2, a.tw, threadIdx.x, kYThreads);
+  __syncthreads();
+  const int grp = threadIdx.x / G, l = threadIdx.x % G;
+  const int j1 = blockIdx.x * ycols<N2>() + grp;
+  const int j = blockIdx.y + a.lvl0;
+  const int run = blockIdx.z >> 1, f0 = 2 * (blockIdx.z & 1);
+  const bool act = j1 < g.K1;
+  const float2* srcA = a.S + ((size_t)(run * 5 + f0) * g.N3 + j) * g.Pp + j1;
+  const float2* srcB = srcA + (size_t)g.N3 * g.Pp;
+  c2x x[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int n2 = l + G * e;
+    int q = -1;
+    if (n2 < g.Ky) q = n2;
+    else if (n2 > N2 - g.Ky) q = n2 - (N2 - g.K2);
+    const bool in = act && q >= 0;
+    const float2 A = in ? srcA[(size_t)q * g.K1] : make_float2(0.f, 0.f);
+    const float2 B = in ? srcB[(size_t)q * g.K1] : make_float2(0.f, 0.f);
+    x[e] = c2x{make_float2(A.x, B.x), make_float2(A.y, B.y)};
+  }
+  reg_fft2<N2, true>(x, fbuf4 + grp * fft2_buf_elems<N2>(), tw4, tw2, l);
+  if (act) {
+    float2* dA = a.mixin + ((size_t)(run * 4 + f0) * g.N3 + j) * N2 * g.K1 + j1;
+    float2* dB = dA + (size_t)g.N3 * N2 * g.K1;
+#pragma unroll
+    for (int sl = 0; sl < E; sl++) {
+      const size_t o = (size_t)reg_fft_out_index<N2>(l, sl) * g.K1;
+      dA[o] = make_float2(x[sl].re.x, x[sl].im.x);
+      dB[o] = make_float2(x[sl].re.y, x[sl].im.y);
+    }
+  }
+}
+
 // mixed combos (C_f, C_fy) [y][j1] -> r_f[q][j1] = Fy(C_f) + i ky Fy(C_fy)
 template <int N2>
 __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
-  constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E, BUF = fft_buf_stride<N2>();
+  constexpr int G = FFTShape<N2>::G, E = FFTShape<N2>::E;
   const Geo g = a.g;
-  __shared__ float2 fbuf[(kYThreads / G) * BUF];
+  __shared__ float4 fbuf4[(kYThreads / G) * fft2_buf_elems<N2>()];
+  __shared__ float4 tw4[E * G];
+  __shared__ float2 tw2[E * G];
+  fill_tw2<N2>(tw4, tw2, a.tw, threadIdx.x, kYThreads);
+  __syncthreads();
   const int grp = threadIdx.x / G, l = threadIdx.x % G;
   const int j1 = blockIdx.x * ycols<N2>() + grp;
   const int j = blockIdx.y + a.lvl0;
@@ -78,16 +127,15 @@ __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
   const bool act = j1 < g.K1;
   const float2* cA = a.mixout + ((size_t)(run * 8 + 2 * f) * g.N3 + j) * N2 * g.K1 + j1;
   const float2* cB = a.mixout + ((size_t)(run * 8 + 2 * f + 1) * g.N3 + j) * N2 * g.K1 + j1;
-  float2 xa[E], xb[E];
+  // (C_f, C_fy) as one packed pair of transforms (sf_fft2.cuh)
+  c2x x[E];
 #pragma unroll
   for (int e = 0; e < E; e++) {
     const size_t o = (size_t)(l + G * e) * g.K1;
-    xa[e] = act ? cA[o] : make_float2(0.f, 0.f);
-    xb[e] = act ? cB[o] : make_float2(0.f, 0.f);
+    const float2 A = act ? cA[o] : make_float2(0.f, 0.f), B = act ? cB[o] : make_float2(0.f, 0.f);
+    x[e] = c2x{make_float2(A.x, B.x), make_float2(A.y, B.y)};
   }
-  float2* buf = fbuf + grp * BUF;
-  reg_fft<N2, false>(xa, buf, a.tw, l);
-  reg_fft<N2, false>(xb, buf, a.tw, l);
+  reg_fft2<N2, false>(x, fbuf4 + grp * fft2_buf_elems<N2>(), tw4, tw2, l);
   if (act) {
     float2* dst = a.rnl + ((size_t)(run * 4 + f) * g.N3 + j) * g.Pp + j1;
 #pragma unroll
@@ -96,7 +144,10 @@ __global__ void __launch_bounds__(kYThreads) k_fft_y(StageArgs a) {
       int q = -1;
       if (n2 < g.Ky) q = n2;
       else if (n2 > N2 - g.Ky) q = n2 - (N2 - g.K2);
-      if (q >= 0) dst[(size_t)q * g.K1] = cadd(xa[sl], cik(a.ky[q], xb[sl]));
+      if (q >= 0) {   // Fy(C_f) + i ky Fy(C_fy)
+        const float ky = a.ky[q];
+        dst[(size_t)q * g.K1] = make_float2(x[sl].re.x - ky * x[sl].im.y, x[sl].im.x + ky * x[sl].re.y);
+      }
     }
   }
 }
@@ -1385,7 +1436,10 @@ static int launch_xpass(const StageArgs& a, cudaStream_t st) {
 template <int N2>
 static void ify_launch(const StageArgs& a, int nz, cudaStream_t st) {
   const int nl = a.nlvl > 0 ? a.nlvl : a.g.N3 - a.lvl0;
-  k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), nl, nz), kYThreads, 0, st>>>(a);
+  if (nz % 4 == 0)   // whole runs: the fields in packed pairs
+    k_ifft_y2<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), nl, nz / 2), kYThreads, 0, st>>>(a);
+  else
+    k_ifft_y<N2><<<dim3(cdiv(a.g.K1, ycols<N2>()), nl, nz), kYThreads, 0, st>>>(a);
 }
 template <int N2>
 static void fy_launch(const StageArgs& a, cudaStream_t st) {

@@ -759,10 +759,13 @@ int sf_profile_step(sf_solver* s, int nsteps, int linear, int cap, double* ms, i
 int sf_profile_names(sf_solver* s, char* buf, size_t len) {
   if (!s || !buf || len == 0) return fail(SF_EINVAL, "bad argument");
   std::string out;
+  // the nonlinear 3D x pass runs as k_xmarch where the solver takes it
+  const bool march = s->xkernel == 1 && !s->tlm && xmarch_supported(stage_args(s, 0, s->cur, false));
   for (int k = 0; k < 3; k++)
     for (int i = 0; i < stage_kernel_count(s->g); i++) {
       if (!out.empty()) out += ",";
-      out += stage_kernel_name(s->g, i);
+      const std::string nm = stage_kernel_name(s->g, i);
+      out += (march && nm == "k_xpass") ? std::string("k_xmarch") : nm;
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);

@@ -37,7 +37,7 @@ def test_bench_reads_the_dominant_kernels_traffic():
     import sys
     sys.path.insert(0, ROOT)
     import bench
-    t = bench.ncu_traffic("shear3d", "k_xpass")
+    t = bench.ncu_traffic("shear3d", "k_xmarch")
     assert t is not None and t > 1e8
     assert bench.ncu_traffic("shear3d", "no_such_kernel") is None
 
