@@ -177,7 +177,7 @@ __device__ __forceinline__ void reg_fft2(c2x (&x)[FFTShape<N>::E], float4* buf, 
 // so that lane l holds the values l0 = 0..3 of (k1 = l % 8, m = l / 8 + 4 h),
 // h = 0, 1; two 4-point DFTs over l0. On exit slot h*4 + q holds
 // out[l + 32 h + 64 q], i.e. out[l + 32 j] with j = h + 2q. tw4 / tw2 are the
-// table of fill_tw2_256w: [k1][l], W_256^{l k1}, k1 < 8, l < 32. buf holds
+// table of fill_tw2_256w: [k1][l], W_256^{l k1}, k1 < 8, l < 32; tw2 its second-stage table. buf holds
 // 8 x 33 float4 (padded columns: every access conflict-free).
 __device__ __forceinline__ void fill_tw2_256w(float4* tw4, float2* tw2, const float2* __restrict__ tw, int tid,
                                               int nthr) {
@@ -185,7 +185,14 @@ __device__ __forceinline__ void fill_tw2_256w(float4* tw4, float2* tw2, const fl
     const int k1 = i / 32, l = i - k1 * 32;
     const float2 w = tw[(l * k1) * (kMaxN / 256)];
     tw4[i] = make_float4(w.x, w.x, w.y, w.y);
-    tw2[i] = make_float2(-w.y, -w.y);
+  }
+  // the second stage's W_32^{l0 m} = W_256^{8 l0 m} as [m][l0], so that the
+  // four distinct entries one warp reads lie in 64 contiguous bytes
+  float4* t2 = reinterpret_cast<float4*>(tw2);
+  for (int i = tid; i < 8 * 4; i += nthr) {
+    const int m = i / 4, l0 = i - m * 4;
+    const float2 w = tw[(8 * l0 * m) * (kMaxN / 256)];
+    t2[i] = make_float4(w.x, w.x, w.y, w.y);
   }
 }
 
@@ -216,7 +223,7 @@ __device__ __forceinline__ void reg_fft2_256w(c2x (&x)[8], float4* buf, const fl
   __syncwarp();
   dft2<8, INV>(x);
 #pragma unroll
-  for (int m = 1; m < 8; m++) tw2_apply<INV>(x[m], tw4 + m * 32 + 8 * l0, tw2 + m * 32 + 8 * l0);
+  for (int m = 1; m < 8; m++) tw2_apply<INV>(x[m], reinterpret_cast<const float4*>(tw2) + m * 4 + l0, tw2);
 #pragma unroll
   for (int m = 0; m < 8; m++) buf[m * 33 + l] = c2x_to4(x[m]);         // element (lane l, m)
   __syncwarp();
