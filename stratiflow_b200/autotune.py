@@ -14,6 +14,8 @@ kernels' launch shapes, which change no result (or only its rounding):
             neighbouring bands' x passes (sf_set_xy_bands; 3D only)
   z_chunks  z-chunks per block of the z solves (sf_set_z_chunks; 0 = the
             launcher's choice from the grid size)
+  xkernel   the 3D nonlinear x pass as level-marching warps (1) or slab
+            blocks (0) (sf_set_xpass_kernel; 3D only)
 
 The search is coordinate descent from the launchers' defaults: each setting
 in turn takes every candidate value with the others held, and a value
@@ -29,8 +31,8 @@ import os
 import time
 from typing import Callable, Dict, List, Tuple
 
-DEFAULTS = {"xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0}
-ORDER = ("xy_bands", "xslabs", "xgroups", "z_chunks")
+DEFAULTS = {"xkernel": 1, "xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0}
+ORDER = ("xkernel", "xy_bands", "xslabs", "xgroups", "z_chunks")
 MARGIN = 0.02   # a candidate must be 2% faster to replace the current value
 
 _memory: Dict[str, dict] = {}
@@ -39,6 +41,7 @@ _memory: Dict[str, dict] = {}
 def space(N2: int, N3: int) -> Dict[str, List[int]]:
     """Candidate values of each setting for a grid."""
     return {
+        "xkernel": [1, 0] if N2 > 1 else [DEFAULTS["xkernel"]],
         "xy_bands": [1, 2, 3, 4, 6, 8] if N2 > 1 else [DEFAULTS["xy_bands"]],
         "xslabs": [0, 1, 2, 3, 4, 6, 8],
         "z_chunks": [0] + [c for c in (8, 16) if N3 >= 2 * c],
@@ -125,6 +128,7 @@ def lookup(key: str, path: str | None = None) -> dict | None:
 
 
 def apply(solver, settings: dict) -> None:
+    solver.set_xpass_kernel(int(settings.get("xkernel", DEFAULTS["xkernel"])))
     solver.set_xpass_slabs(int(settings["xslabs"]))
     if solver.N2 > 1:
         solver.set_xy_bands(int(settings["xy_bands"]))
