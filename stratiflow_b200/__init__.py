@@ -36,7 +36,7 @@ EXPORTS = [
     "sf_vecs_zero_pressure", "sf_vecs_synchronize", "sf_set_tangent",
     "sf_net_create", "sf_net_destroy", "sf_net_num_params", "sf_net_get_params", "sf_net_set_params",
     "sf_net_forward", "sf_net_set_data", "sf_net_gradient", "sf_net_train",
-    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_xy_bands", "sf_set_z_chunks", "sf_set_xpass_groups", "sf_set_xpass_kernel",
+    "sf_vecs_gram", "sf_vecs_update", "sf_vecs_band", "sf_vecs_column", "sf_set_xpass_slabs", "sf_set_xy_bands", "sf_set_z_chunks", "sf_set_xpass_groups", "sf_set_xpass_kernel", "sf_set_z_kernel",
     "sf_ensemble_create", "sf_ensemble_destroy", "sf_ensemble_member", "sf_ensemble_step",
     "sf_ensemble_synchronize", "sf_ensemble_launch_count", "sf_ensemble_stream", "sf_ensemble_profile", "sf_set_base_device",
     "sf_get_nodal", "sf_set_nodal", "sf_velocity_maxima", "sf_cfl", "sf_get_dt", "sf_get_runs", "sf_step_adjoint",
@@ -96,7 +96,7 @@ def load_library(path: str | None = None):
         "sf_net_set_params": [vp, fp], "sf_net_forward": [vp, fp, i, fp], "sf_net_set_data": [vp, fp, fp, i],
         "sf_net_gradient": [vp, fp, dp], "sf_net_train": [vp, i, d, dp],
         "sf_vecs_gram": [vp, i, i, vp, i, i, d, dp], "sf_vecs_update": [vp, i, i, d, vp, i, i, dp],
-        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_xy_bands": [vp, i], "sf_set_z_chunks": [vp, i], "sf_set_xpass_groups": [vp, i], "sf_set_xpass_kernel": [vp, i], "sf_set_base_device": [vp, i, vp],
+        "sf_vecs_band": [vp, i, i, i, i], "sf_vecs_column": [vp, i, i, i, fp, i], "sf_set_xpass_slabs": [vp, i], "sf_set_xy_bands": [vp, i], "sf_set_z_chunks": [vp, i], "sf_set_xpass_groups": [vp, i], "sf_set_xpass_kernel": [vp, i], "sf_set_z_kernel": [vp, i], "sf_set_base_device": [vp, i, vp],
         "sf_get_nodal": [vp, i, i, fp], "sf_set_nodal": [vp, i, i, fp], "sf_velocity_maxima": [vp, i, dp],
         "sf_cfl": [vp, i, dp], "sf_get_dt": [vp, dp], "sf_get_runs": [vp, C.POINTER(i)],
         "sf_step_adjoint": [vp, vp, vp],
@@ -409,6 +409,11 @@ class IMEXRK:
         """3D nonlinear x pass: 1 level-marching lane groups (default), 0 slab
         blocks; a launch setting (the results change only by rounding)."""
         _check(load_library().sf_set_xpass_kernel(self._h, int(kind)))
+
+    def set_z_kernel(self, kind):
+        """z pass: 0 k_z_step (default), 1 k_z_step_tma (TMA-fed first
+        sweeps); a launch setting (the same arithmetic in the same order)."""
+        _check(load_library().sf_set_z_kernel(self._h, int(kind)))
 
     def set_z_chunks(self, chunks):
         """z chunks per block of the z solves (0: automatic, 8 or 16); a

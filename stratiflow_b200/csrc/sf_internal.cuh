@@ -84,6 +84,20 @@ struct StageArgs {
   int zchunks;      // z chunks per block of the z solves (8 or 16; 0: chosen by the launcher)
   int xgroups;      // lane groups per x-pass block (0: chosen by the launcher)
   int xkernel;      // 3D nonlinear x pass: 1 level-marching lane groups (k_xmarch), 0 slab blocks (k_xpass)
+  int zkernel;      // z pass: 0 k_z_step, 1 k_z_step_tma (inputs by the tensor-memory accelerator)
+  const void* zmaps;   // host ZMaps of the solver (k_z_step_tma), or null
+  int* zerr;           // device word set by a k_z_step_tma wait that ran out
+};
+
+// the tensor maps of k_z_step_tma's inputs (each the bytes of one
+// CUtensorMap), encoded once per solver, and the state buffers they view
+struct alignas(64) ZMap {
+  unsigned char bytes[128];
+};
+struct ZMaps {
+  ZMap s[2], rnl, rold, iden;
+  const void* sbase[2];
+  const void* rbase[3];   // rnl, rold, inv_den
 };
 
 // side streams and events of the banded 3D x-y pass: the inverse y
@@ -107,6 +121,13 @@ constexpr int kEnsThreads = 256;
 
 // launchers (sf_kernels.cu); each returns the number of kernels launched
 int prepare_kernels();
+// the z pass with TMA-fed first sweeps (sf_zstep.cu)
+bool zstep_tma_supported(const Geo& g);
+int zstep_tma_maps(const Geo& g, const float2* S0, const float2* S1, const float2* rnl, const float2* rold,
+                   const float* inv_den, ZMaps* out);
+int launch_z_step_tma(const StageArgs& a, cudaStream_t st);
+bool z_step_takes_tma(const StageArgs& a);
+int prepare_zstep_tma_kernels();
 // the 3D nonlinear x pass as level-marching lane groups (sf_xmarch.cu): levels
 // t_lo .. t_hi - 1 of every run and y row
 bool xmarch_supported(const StageArgs& a);

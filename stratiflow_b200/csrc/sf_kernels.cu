@@ -1484,6 +1484,7 @@ int prepare_kernels() {
   ATTR((k_z_step<8, false>)) ATTR((k_z_step<8, true>)) ATTR((k_z_step<16, false>)) ATTR((k_z_step<16, true>))
 #undef ATTR
   if (e == cudaSuccess && prepare_xmarch_kernels() != 0) return -1;
+  if (e == cudaSuccess && prepare_zstep_tma_kernels() != 0) return -1;
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -1512,10 +1513,18 @@ int launch_project(const StageArgs& a, cudaStream_t st) {
 // chunks of 48 levels or more take the variant with end-test-free interior
 // sweeps (measured 7% faster at 384 levels in 8 chunks, and slower with
 // 32-level chunks, where it is not used)
+// the z pass as k_z_step_tma: where the solver asks for it, has its tensor
+// maps, and the launch takes 8 chunks
+bool z_step_takes_tma(const StageArgs& a) {
+  const int zw = a.zchunks ? a.zchunks : z_chunks(a.g, 1);
+  return a.zkernel == 1 && a.zmaps && zw == 8 && zstep_tma_supported(a.g);
+}
+
 static void launch_z_step(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
   const dim3 zgrid(cdiv(g.P, 16), 1, g.nrun);
   const int zw = a.zchunks ? a.zchunks : z_chunks(g, 1);
+  if (z_step_takes_tma(a) && launch_z_step_tma(a, st)) return;
   const bool ic = cdiv(g.N3, zw) >= 48;
   if (zw == 16) {
     if (ic) k_z_step<16, true><<<zgrid, 16 * 32, zchunk_smem(g, 16), st>>>(a);

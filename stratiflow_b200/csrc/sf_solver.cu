@@ -59,6 +59,9 @@ struct sf_solver {
   int zchunks = 0;               // z chunks per z-solve block (sf_set_z_chunks)
   int xgroups = 0;               // lane groups per x-pass block (sf_set_xpass_groups)
   int xkernel = 1;               // 3D nonlinear x pass: 1 level-marching, 0 slab blocks (sf_set_xpass_kernel)
+  int zkernel = 0;               // z pass: 0 k_z_step, 1 k_z_step_tma (sf_set_z_kernel)
+  ZMaps* zmaps = nullptr;        // tensor maps of k_z_step_tma's inputs (null: not supported here)
+  int* zerr = nullptr;           // set on the device by a k_z_step_tma wait that ran out
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
   long long launches = 0;
   long long launches_per_step[2] = {0, 0};
@@ -98,7 +101,9 @@ static void free_all(sf_solver* s) {
   for (int l = 0; l < 2; l++)
     for (int p = 0; p < 2; p++)
       if (s->graph[l][p]) cudaGraphExecDestroy(s->graph[l][p]);
-  void* ptrs[] = {s->amix, s->adir, s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
+  delete s->zmaps;
+  s->zmaps = nullptr;
+  void* ptrs[] = {s->zerr, s->amix, s->adir, s->S[0], s->S[1], s->rold, s->rnl, s->qbuf, s->mixin, s->mixout, s->base, s->zc, s->fa,
                   s->fc, s->inv_den, s->kx, s->ky, s->Ri, s->Ubar, s->dBdz, s->bands, s->kxd, s->kyd,
                   s->red, s->tw, s->stage_ref};
   for (void* p : ptrs)
@@ -223,6 +228,9 @@ static StageArgs stage_args(sf_solver* s, int k, int cur, bool linear) {
   a.zchunks = s->zchunks;
   a.xgroups = s->xgroups;
   a.xkernel = s->xkernel;
+  a.zkernel = s->zkernel;
+  a.zmaps = s->zmaps;
+  a.zerr = s->zerr;
   const float h = s->h[k];
   a.h = h;
   a.hz = h * (float)kZeta[k];   // (h[k]*zeta[k]) in stratifloat
@@ -445,6 +453,15 @@ int sf_create(const sf_grid* grid, const sf_flow* flow, double dt, int device, s
   {
     std::vector<float> ones((size_t)nrun * N3, 1.f);
     CKC(cudaMemcpy(s->dBdz, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice));
+  }
+  CKC(cudaMalloc(&s->zerr, sizeof(int)));
+  CKC(cudaMemset(s->zerr, 0, sizeof(int)));
+  if (zstep_tma_supported(g)) {
+    s->zmaps = new ZMaps();
+    if (zstep_tma_maps(g, s->S[0], s->S[1], s->rnl, s->rold, s->inv_den, s->zmaps) != 0) {
+      delete s->zmaps;   // no tensor maps: k_z_step serves every launch
+      s->zmaps = nullptr;
+    }
   }
   int rc = refactor(s);
   if (rc != SF_OK) return cleanup_fail(rc);
@@ -761,11 +778,13 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
   std::string out;
   // the nonlinear 3D x pass runs as k_xmarch where the solver takes it
   const bool march = s->xkernel == 1 && !s->tlm && xmarch_supported(stage_args(s, 0, s->cur, false));
+  // and the z pass as k_z_step_tma
+  const bool ztma = z_step_takes_tma(stage_args(s, 0, s->cur, false));
   for (int k = 0; k < 3; k++)
     for (int i = 0; i < stage_kernel_count(s->g); i++) {
       if (!out.empty()) out += ",";
       const std::string nm = stage_kernel_name(s->g, i);
-      out += (march && nm == "k_xpass") ? std::string("k_xmarch") : nm;
+      out += (march && nm == "k_xpass") ? std::string("k_xmarch") : (ztma && nm == "k_z_step") ? std::string("k_z_step_tma") : nm;
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);
@@ -841,6 +860,15 @@ int sf_set_xpass_kernel(sf_solver* s, int kind) {
   return SF_OK;
 }
 
+int sf_set_z_kernel(sf_solver* s, int kind) {
+  if (!s || (kind != 0 && kind != 1)) return fail(SF_EINVAL, "kind must be 0 or 1");
+  if (kind != s->zkernel) {
+    s->zkernel = kind;
+    drop_graphs(s);
+  }
+  return SF_OK;
+}
+
 int sf_set_z_chunks(sf_solver* s, int chunks) {
   if (!s || !(chunks == 0 || chunks == 8 || chunks == 16)) return fail(SF_EINVAL, "chunks must be 0, 8 or 16");
   if (s->g.N3 < 2 * (chunks ? chunks : 8)) return fail(SF_EINVAL, "too few levels for that many chunks");
@@ -886,6 +914,14 @@ int sf_synchronize(sf_solver* s) {
   if (s->pipe) {
     CK(cudaStreamSynchronize(s->pipe->h2d));
     CK(cudaStreamSynchronize(s->pipe->d2h));
+  }
+  if (s->zkernel == 1 && s->zmaps) {
+    int h = 0;
+    CK(cudaMemcpy(&h, s->zerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+      CK(cudaMemset(s->zerr, 0, sizeof(int)));
+      return fail(SF_ECUDA, "a z-pass block gave up waiting for its input tiles");
+    }
   }
   return SF_OK;
 }

@@ -17,22 +17,22 @@ def _cost(best, base=1.0, step=0.1):
 
 
 def test_search_finds_the_fastest_settings():
-    best = {"xkernel": 0, "xy_bands": 6, "xslabs": 2, "z_chunks": 16, "xgroups": 16}
+    best = {"xkernel": 0, "xy_bands": 6, "xslabs": 2, "z_chunks": 16, "xgroups": 16, "zkernel": 1}
     got, log = A.search(_cost(best), A.space(128, 384))
     assert got == best
-    assert log[0][0] == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0}   # starts from the defaults
+    assert log[0][0] == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0}   # starts from the defaults
 
 
 def test_search_keeps_the_default_within_the_noise_margin():
     def measure(s):   # every other value is 1% faster: not enough to switch
-        return 0.99 if s != {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0} else 1.0
+        return 0.99 if s != {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0} else 1.0
     got, _ = A.search(measure, A.space(128, 384))
-    assert got == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0}
+    assert got == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0}
 
 
 def test_each_setting_is_measured_once():
     calls = []
-    best = {"xkernel": 1, "xy_bands": 2, "xslabs": 6, "z_chunks": 8, "xgroups": 8}
+    best = {"xkernel": 1, "xy_bands": 2, "xslabs": 6, "z_chunks": 8, "xgroups": 8, "zkernel": 0}
     f = _cost(best)
     A.search(lambda s: (calls.append(tuple(sorted(s.items()))), f(s))[1], A.space(128, 384))
     assert len(calls) == len(set(calls))
@@ -52,10 +52,10 @@ def test_plan_cache_round_trip(tmp_path, monkeypatch):
     A._memory.clear()
     key = A.plan_key("B200", 256, 128, 384, 1, "step")
     assert A.lookup(key) is None
-    A.store(key, {"xkernel": 0, "xy_bands": 3, "xslabs": 6, "z_chunks": 8, "xgroups": 16})
+    A.store(key, {"xkernel": 0, "xy_bands": 3, "xslabs": 6, "z_chunks": 8, "xgroups": 16, "zkernel": 1})
     assert json.load(open(path))[key]["xy_bands"] == 3
     A._memory.clear()
-    assert A.lookup(key) == {"xkernel": 0, "xy_bands": 3, "xslabs": 6, "z_chunks": 8, "xgroups": 16}
+    assert A.lookup(key) == {"xkernel": 0, "xy_bands": 3, "xslabs": 6, "z_chunks": 8, "xgroups": 16, "zkernel": 1}
 
 
 class _FakeSolver:
@@ -70,6 +70,7 @@ class _FakeSolver:
     def set_xy_bands(self, v): self.applied["xy_bands"] = v
     def set_z_chunks(self, v): self.applied["z_chunks"] = v
     def set_xpass_groups(self, v): self.applied["xgroups"] = v
+    def set_z_kernel(self, v): self.applied["zkernel"] = v
     def get_state_kept(self): return self.state
     def set_state_kept(self, st): assert st is self.state
     def TimeStep(self, n=1): pass
