@@ -45,27 +45,25 @@ __device__ __forceinline__ uint32_t zs(const void* p) { return (uint32_t)__cvta_
 __device__ __forceinline__ void mb_init(uint64_t* b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(zs(b)), "r"(count) : "memory");
 }
-__device__ __forceinline__ void mb_expect_tx(uint64_t* b, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(zs(b)), "r"(bytes) : "memory");
+__device__ __forceinline__ bool mb_try(uint32_t b, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(b), "r"(parity)
+      : "memory");
+  return ok != 0;
 }
-__device__ __forceinline__ void mb_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(zs(b)) : "memory");
-}
-// wait for the phase of the given parity to complete, for at most `limit`
-// SM cycles; a wait that runs out sets the block's `bad` word (after which the
-// block's other waits give up at once, unless `drain`) and the solver's error
-// word, and returns
-__device__ __forceinline__ void mb_wait(uint64_t* b, unsigned parity, int* err, int code, volatile int* bad,
+// wait for the phase of the given parity of the barrier at shared address b
+// to complete, for at most `limit` SM cycles; a wait that runs out sets the
+// block's `bad` word (after which the block's other waits give up at once,
+// unless `drain`) and the solver's error word, and returns
+__device__ __forceinline__ void mb_wait(uint32_t b, unsigned parity, int* err, int code, volatile int* bad,
                                         long long limit = kZWaitCycles, bool drain = false) {
+  if (mb_try(b, parity)) return;
   const long long t0 = clock64();
   for (;;) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(zs(b)), "r"(parity)
-        : "memory");
-    if (ok) return;
+    if (mb_try(b, parity)) return;
     if (!drain && *bad) return;
     if (clock64() - t0 > limit) {
       *bad = 1;
@@ -74,19 +72,14 @@ __device__ __forceinline__ void mb_wait(uint64_t* b, unsigned parity, int* err, 
     }
   }
 }
-// one tile of a 2D tensor map (box: columns x kZTL rows) into shared memory
-__device__ __forceinline__ void tma2(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-          zs(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(zs(bar))
-      : "memory");
-}
 // the block's barrier for the chunk scans
 __device__ __forceinline__ void zc_sync() { asm volatile("bar.sync 1, %0;" ::"n"(kZW * 32) : "memory"); }
 
-__device__ __forceinline__ void tz_st1(uint32_t addr, float v) {
-  asm volatile("tcgen05.st.sync.aligned.32x32b.x1.b32 [%0], {%1};" ::"r"(addr), "f"(v) : "memory");
+__device__ __forceinline__ void tz_st4(uint32_t addr, const float (&v)[kZTL]) {
+  static_assert(kZTL == 4, "one 4-column store per tile");
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v[0]), "f"(v[1]),
+               "f"(v[2]), "f"(v[3])
+               : "memory");
 }
 __device__ __forceinline__ void tz_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tz_ld16(uint32_t addr, float (&v)[16]) {
@@ -159,46 +152,59 @@ struct ZTmaps {
 
 // a warp's ring: fill k (the k-th tile the warp reads) goes to slot k % kZNS;
 // fills are numbered through the systems in order (u1, [u2], u3, b, the
-// projection), nt tiles each
+// projection), nt tiles each. Every lane keeps the same copy of the
+// counters; lane 0 issues the copies.
 struct ZRing {
   float* slots;
-  uint64_t* full;
-  int kc;        // fills read
-  int issued;    // fills issued
-  int nt;        // tiles per system of this chunk
-  int nsys;      // systems (4 in 3D, 3 in 2D, the projection included)
+  uint32_t sbase, bbase;   // shared addresses of slot 0 and of its barrier
+  int kslot, kpar;         // slot and phase parity of the next fill to read
+  int kc;                  // fills read
+  int issued;              // fills issued
+  int islot, it, isys;     // slot, tile and system of the next fill to issue
+  int nt;                  // tiles per system of this chunk
 };
 
-// issue fill k (lane 0)
-__device__ __forceinline__ void zr_issue(const StageArgs& a, const ZRing& R, const ZTmaps& M, int k, int js) {
+__device__ __forceinline__ void tma2s(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+__device__ __forceinline__ void mb_expect_tx_s(uint32_t bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// issue the next fill (lane 0): the tile of levels js + 4 it .. + 3 of every
+// input of system isys
+__device__ __forceinline__ void zr_issue(const StageArgs& a, const ZRing& R, const ZTmaps& M, int js) {
   const Geo& g = a.g;
   const int N3 = g.N3, run = blockIdx.z;
   const int x32 = 32 * blockIdx.x, x16 = 16 * blockIdx.x;
   const bool use_rold = a.hz != 0.f;
-  const int si = k / R.nt, t = k - si * R.nt;
-  const int sys = g.dim3 ? si : (si == 0 ? 0 : si + 1);   // 0 u1, 1 u2, 2 u3, 3 b, 4 projection
-  const int f = sys < 4 ? sys : 0;
-  const int fam = sys < 2 ? 0 : (sys == 2 ? 1 : 2);
-  const int fs = (fam == 2 ? 1 : (fam == 1 ? 2 : 0)) * 3 + a.stage;
-  const int slot = k % kZNS;
-  uint64_t* bar = R.full + slot;
-  float* r = R.slots + (size_t)slot * kZSlotFloats;
-  const int j = js + t * kZTL;   // the tile's first level
-  mb_expect_tx(bar, zt_tiles(sys, use_rold, g.dim3 != 0).bytes);
-  auto at = [&](int arr) { return r + arr * kZTL * 32; };
+  const int sys = g.dim3 ? R.isys : (R.isys == 0 ? 0 : R.isys + 1);   // 0 u1, 1 u2, 2 u3, 3 b, 4 projection
+  const uint32_t bar = R.bbase + 8u * R.islot;
+  const uint32_t r = R.sbase + (uint32_t)(R.islot * kZSlotFloats * 4);
+  const uint32_t ri = r + kZIden * 4;
+  constexpr uint32_t A = kZTL * 32 * 4;   // bytes of one full-width tile
+  const int j = js + R.it * kZTL;         // the tile's first level
+  const int s5 = run * 5 * N3 + j, s4 = run * 4 * N3 + j;
+  mb_expect_tx_s(bar, zt_tiles(sys, use_rold, g.dim3 != 0).bytes);
   if (sys < 4) {
-    tma2(at(0), M.S, x32, (run * 5 + f) * N3 + j + 1, bar);                       // u_{j+1}
-    tma2(at(1), M.R, x32, (run * 4 + f) * N3 + j, bar);                           // r
-    if (use_rold) tma2(at(2), M.O, x32, (run * 4 + f) * N3 + j, bar);             // r_old
-    tma2(r + kZIden, M.I, x16, fs * N3 + j, bar);                                 // 1/den
-    if (fam == 0 || fam == 1) tma2(at(3), M.S, x32, (run * 5 + 4) * N3 + j, bar);   // p
-    if (fam == 1) tma2(at(4), M.S, x32, (run * 5 + 3) * N3 + j, bar);             // b
-    if (fam == 2) tma2(at(3), M.S, x32, (run * 5 + 2) * N3 + j + 1, bar);         // u3_{j+1}
+    const int fam = sys < 2 ? 0 : (sys == 2 ? 1 : 2);
+    const int fs = (fam == 2 ? 1 : (fam == 1 ? 2 : 0)) * 3 + a.stage;
+    tma2s(r, M.S, x32, s5 + sys * N3 + 1, bar);                        // u_{j+1}
+    tma2s(r + A, M.R, x32, s4 + sys * N3, bar);                        // r
+    if (use_rold) tma2s(r + 2 * A, M.O, x32, s4 + sys * N3, bar);      // r_old
+    tma2s(ri, M.I, x16, fs * N3 + j, bar);                             // 1/den
+    if (fam < 2) tma2s(r + 3 * A, M.S, x32, s5 + 4 * N3, bar);         // p
+    if (fam == 1) tma2s(r + 4 * A, M.S, x32, s5 + 3 * N3, bar);        // b
+    if (fam == 2) tma2s(r + 3 * A, M.S, x32, s5 + 2 * N3 + 1, bar);    // u3_{j+1}
   } else {
-    tma2(at(0), M.Sn, x32, (run * 5 + 0) * N3 + j, bar);                          // u1 (new)
-    if (g.dim3) tma2(at(1), M.Sn, x32, (run * 5 + 1) * N3 + j, bar);              // u2 (new)
-    tma2(at(2), M.Sn, x32, (run * 5 + 2) * N3 + j + 1, bar);                      // u3_{j+1} (new)
-    tma2(r + kZIden, M.I, x16, kFS_Lap * N3 + j, bar);                            // 1/den of the Laplacian
+    tma2s(r, M.Sn, x32, s5, bar);                                      // u1 (new)
+    if (g.dim3) tma2s(r + A, M.Sn, x32, s5 + N3, bar);                 // u2 (new)
+    tma2s(r + 2 * A, M.Sn, x32, s5 + 2 * N3 + 1, bar);                 // u3_{j+1} (new)
+    tma2s(ri, M.I, x16, kFS_Lap * N3 + j, bar);                        // 1/den of the Laplacian
   }
 }
 
@@ -210,24 +216,31 @@ __device__ __forceinline__ void zr_top_up(const StageArgs& a, ZRing& R, const ZT
   const int target = min(R.kc + kZNS, allowed);
   if (target <= R.issued) return;
   __syncwarp();
-  if (lane == 0) {
-    // the warp's reads of the slots are ordered before the copies that overwrite them
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    for (int k = R.issued; k < target; k++) zr_issue(a, R, M, k, js);
+  if (lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // reads before the overwrite
+  while (R.issued < target) {
+    if (lane == 0) zr_issue(a, R, M, js);
+    R.issued++;
+    R.islot = R.islot == kZNS - 1 ? 0 : R.islot + 1;
+    if (++R.it == R.nt) {
+      R.it = 0;
+      R.isys++;
+    }
   }
-  R.issued = target;
 }
 
 // the warp's wait for its next fill; returns the slot's floats
 __device__ __forceinline__ const float* zr_take(const StageArgs& a, ZShared& sh, ZRing& R) {
-  const int k = R.kc;
-  mb_wait(R.full + k % kZNS, (k / kZNS) & 1, a.zerr, 1, &sh.bad);
-  return R.slots + (size_t)(k % kZNS) * kZSlotFloats;
+  mb_wait(R.bbase + 8u * R.kslot, R.kpar, a.zerr, 1, &sh.bad);
+  return R.slots + R.kslot * kZSlotFloats;
 }
 // after the warp has read the fill: the next fills into the freed slot
 __device__ __forceinline__ void zr_done(const StageArgs& a, ZRing& R, const ZTmaps& M, int allowed, int js,
                                         int lane) {
   R.kc++;
+  if (++R.kslot == kZNS) {
+    R.kslot = 0;
+    R.kpar ^= 1;
+  }
   zr_top_up(a, R, M, allowed, js, lane);
 }
 
@@ -327,6 +340,7 @@ __device__ __forceinline__ void zt_cn(const StageArgs& a, ZShared& sh, ZRing& R,
     constexpr bool IN = decltype(tag)::value;
     for (int t0 = js; t0 < je; t0 += kZTL) {
       const float* r = zr_take(a, sh, R);
+      float bev[kZTL] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
       for (int i = 0; i < kZTL; i++) {
         const int j = t0 + i;
@@ -362,13 +376,14 @@ __device__ __forceinline__ void zt_cn(const StageArgs& a, ZShared& sh, ZRing& R,
         if (zend) rhs = 0.f;
         const float be = rhs * bi;
         const float al = (!IN && j == 0) ? 0.f : -fa[j] * bi;
-        tz_st1(tc + (uint32_t)(j - js), be);
+        bev[i] = be;
         if (act) rold[j * S2] = rt;
         A = al * A;
         B = al * B + be;
         um = u0;
         u0 = up;
       }
+      tz_st4(tc + (uint32_t)(t0 - js), bev);
       zr_done(a, R, M, allowed, js, lane);
     }
   };
@@ -435,6 +450,7 @@ __device__ __forceinline__ void zt_proj(const StageArgs& a, ZShared& sh, ZRing& 
   float A = 1.f, B = 0.f;
   for (int t0 = js; t0 < je; t0 += kZTL) {
     const float* r = zr_take(a, sh, R);
+    float bev[kZTL] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
     for (int i = 0; i < kZTL; i++) {
       const int j = t0 + i;
@@ -447,11 +463,12 @@ __device__ __forceinline__ void zt_proj(const StageArgs& a, ZShared& sh, ZRing& 
       if (j >= 2 && j <= N3 - 3) dv = sc * (kxv * b1 + kyv * b2) + (ddn_di[j] * w0 + ddn_up[j] * w1);
       const float be = dv * bi;
       const float al = (j == 0) ? 0.f : -a_[j] * bi;
-      tz_st1(tc + (uint32_t)(j - js), be);
+      bev[i] = be;
       A = al * A;
       B = al * B + be;
       w0 = w1;
     }
+    tz_st4(tc + (uint32_t)(t0 - js), bev);
     zr_done(a, R, M, allowed, js, lane);
   }
   auto Cof = [&](int j, float bij) {   // the (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
@@ -532,12 +549,18 @@ __global__ void __launch_bounds__(kZThreads, 3)
   zt_chunk(a.g.N3, w, js, je);
   ZRing R;
   R.slots = rings + (size_t)w * kZNS * kZSlotFloats;
-  R.full = sh.full[w];
+  R.sbase = zs(R.slots);
+  R.bbase = zs(&sh.full[w][0]);
+  R.kslot = 0;
+  R.kpar = 0;
   R.kc = 0;
   R.issued = 0;
+  R.islot = 0;
+  R.it = 0;
+  R.isys = 0;
   R.nt = (je - js + kZTL - 1) / kZTL;
-  R.nsys = dim3 ? 5 : 4;
-  const int ncn = (R.nsys - 1) * R.nt, ntot = R.nsys * R.nt;
+  const int nsys = dim3 ? 5 : 4;
+  const int ncn = (nsys - 1) * R.nt, ntot = nsys * R.nt;
   zr_top_up(a, R, M, ncn, js, lane);
   const uint32_t tc = sh.tmem_base + ((uint32_t)(32 * (w & 3)) << 16) + (uint32_t)((w >> 2) * kZTCols);
   zt_cn<0>(a, sh, R, M, ncn, 0, tc);
@@ -555,7 +578,7 @@ __global__ void __launch_bounds__(kZThreads, 3)
   // unless a wait ran out)
   if (lane == 0)
     for (int k = max(0, R.issued - kZNS); k < R.issued; k++)
-      mb_wait(R.full + k % kZNS, (k / kZNS) & 1, a.zerr, 3, &sh.bad, kZDrainCycles, true);
+      mb_wait(R.bbase + 8u * (k % kZNS), (k / kZNS) & 1, a.zerr, 3, &sh.bad, kZDrainCycles, true);
   __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
