@@ -202,7 +202,7 @@ def kernel_bytes(s, name):
         return (4 * M + 8 * M) if s.dim3 else (3 * S + 3 * S)
     if name == "k_fft_y":
         return 8 * M + 4 * S
-    if name in ("k_z_step", "k_z_step_tma"):
+    if name in ("k_z_step", "k_z_step_tma", "k_z_step_c"):
         # in: u (nf fields), p, r_nl, r_old, and the per-mode factors 1/den_j
         # (float, half a complex field) of the velocity, u3, b and Laplacian
         # systems; out: u, p and r_old for the next stage

@@ -192,14 +192,16 @@ int sf_set_xy_bands(sf_solver* s, int bands);
  * rounding (the chunked solve reassociates the recurrence). */
 int sf_set_z_chunks(sf_solver* s, int chunks);
 
-/* Launch tuning of the z pass (no counterpart in the reference): kind 0 (the
- * default) runs it as k_z_step, whose warps load their own inputs; kind 1 as
- * k_z_step_tma, where a producer warp brings the first sweeps' inputs into
- * shared memory with tensor-memory-accelerator copies and the Thomas
- * intermediates live in tensor memory. Kind 1 applies with 8 z chunks and
- * grids whose kept modes pad to whole groups of 16 (else kind 0 runs); a
- * wait for its tiles that runs out is reported by sf_synchronize. The
- * results are the same arithmetic in the same order. */
+/* Launch tuning of the z pass (no counterpart in the reference): kind 2 (the
+ * default) runs it as k_z_step_c, one lane per complex mode in paired FP32
+ * instructions and two z-chunks per warp (16 chunks per block; grids with
+ * N3 >= 32, else kind 0 runs); kind 0 as k_z_step, one lane per real
+ * component and one chunk per warp; kind 1 as k_z_step_tma, k_z_step with
+ * each warp's first-sweep inputs brought into shared memory by
+ * tensor-memory-accelerator copies and the Thomas intermediates in tensor
+ * memory (with 8 z chunks; a wait for its tiles that runs out is reported by
+ * sf_synchronize). The three solve the same systems with the same terms; the
+ * results differ by rounding (the chunk count reassociates the recurrences). */
 int sf_set_z_kernel(sf_solver* s, int kind);
 
 /* Launch tuning of the x pass (no counterpart in the reference): lane groups

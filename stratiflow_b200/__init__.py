@@ -411,8 +411,9 @@ class IMEXRK:
         _check(load_library().sf_set_xpass_kernel(self._h, int(kind)))
 
     def set_z_kernel(self, kind):
-        """z pass: 0 k_z_step (default), 1 k_z_step_tma (TMA-fed first
-        sweeps); a launch setting (the same arithmetic in the same order)."""
+        """z pass: 2 k_z_step_c (default, one lane per complex mode), 0
+        k_z_step, 1 k_z_step_tma (TMA-fed first sweeps); a launch setting
+        (the results change only by rounding)."""
         _check(load_library().sf_set_z_kernel(self._h, int(kind)))
 
     def set_z_chunks(self, chunks):

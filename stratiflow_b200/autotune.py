@@ -16,9 +16,9 @@ kernels' launch shapes, which change no result (or only its rounding):
             launcher's choice from the grid size)
   xkernel   the 3D nonlinear x pass as level-marching warps (1) or slab
             blocks (0) (sf_set_xpass_kernel; 3D only)
-  zkernel   the z pass as k_z_step (0) or k_z_step_tma (1, inputs brought
-            in by tensor-map copies; applies with 8 z-chunks)
-            (sf_set_z_kernel)
+  zkernel   the z pass as k_z_step_c (2, one lane per complex mode),
+            k_z_step (0) or k_z_step_tma (1, inputs brought in by
+            tensor-map copies; applies with 8 z-chunks) (sf_set_z_kernel)
 
 The search is coordinate descent from the launchers' defaults: each setting
 in turn takes every candidate value with the others held, and a value
@@ -34,7 +34,7 @@ import os
 import time
 from typing import Callable, Dict, List, Tuple
 
-DEFAULTS = {"xkernel": 1, "xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0, "zkernel": 0}
+DEFAULTS = {"xkernel": 1, "xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0, "zkernel": 2}
 ORDER = ("xkernel", "xy_bands", "xslabs", "xgroups", "z_chunks", "zkernel")
 MARGIN = 0.02   # a candidate must be 2% faster to replace the current value
 
@@ -49,7 +49,7 @@ def space(N2: int, N3: int) -> Dict[str, List[int]]:
         "xslabs": [0, 1, 2, 3, 4, 6, 8],
         "z_chunks": [0] + [c for c in (8, 16) if N3 >= 2 * c],
         "xgroups": [0, 8, 16],
-        "zkernel": [0, 1],
+        "zkernel": [2, 0, 1],
     }
 
 
@@ -138,7 +138,7 @@ def apply(solver, settings: dict) -> None:
         solver.set_xy_bands(int(settings["xy_bands"]))
     solver.set_z_chunks(int(settings["z_chunks"]))
     solver.set_xpass_groups(int(settings.get("xgroups", 0)))
-    solver.set_z_kernel(int(settings.get("zkernel", 0)))
+    solver.set_z_kernel(int(settings.get("zkernel", DEFAULTS["zkernel"])))
 
 
 def device_name(solver) -> str:

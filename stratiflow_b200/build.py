@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libstratiflow_b200.so")
-SOURCES = ["sf_solver.cu", "sf_kernels.cu", "sf_noalloc.cu", "sf_vecs.cu", "sf_net.cu", "sf_io.cu", "sf_adjoint.cu", "sf_xmarch.cu", "sf_zstep.cu"]
+SOURCES = ["sf_solver.cu", "sf_kernels.cu", "sf_noalloc.cu", "sf_vecs.cu", "sf_net.cu", "sf_io.cu", "sf_adjoint.cu", "sf_xmarch.cu", "sf_zstep.cu", "sf_zstep2.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

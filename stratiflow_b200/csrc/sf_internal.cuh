@@ -84,7 +84,8 @@ struct StageArgs {
   int zchunks;      // z chunks per block of the z solves (8 or 16; 0: chosen by the launcher)
   int xgroups;      // lane groups per x-pass block (0: chosen by the launcher)
   int xkernel;      // 3D nonlinear x pass: 1 level-marching lane groups (k_xmarch), 0 slab blocks (k_xpass)
-  int zkernel;      // z pass: 0 k_z_step, 1 k_z_step_tma (inputs by the tensor-memory accelerator)
+  int zkernel;      // z pass: 0 k_z_step, 1 k_z_step_tma (inputs by the tensor-memory accelerator),
+                    // 2 k_z_step_c (one lane per complex mode)
   const void* zmaps;   // host ZMaps of the solver (k_z_step_tma), or null
   int* zerr;           // device word set by a k_z_step_tma wait that ran out
 };
@@ -127,6 +128,11 @@ int zstep_tma_maps(const Geo& g, const float2* S0, const float2* S1, const float
                    const float* inv_den, ZMaps* out);
 int launch_z_step_tma(const StageArgs& a, cudaStream_t st);
 bool z_step_takes_tma(const StageArgs& a);
+// the z pass with one lane per complex mode (sf_zstep2.cu)
+bool zstep_c_supported(const Geo& g);
+int launch_z_step_c(const StageArgs& a, cudaStream_t st);
+int prepare_zstep_c_kernels();
+bool z_step_takes_c(const StageArgs& a);
 int prepare_zstep_tma_kernels();
 // the 3D nonlinear x pass as level-marching lane groups (sf_xmarch.cu): levels
 // t_lo .. t_hi - 1 of every run and y row

@@ -1485,6 +1485,7 @@ int prepare_kernels() {
 #undef ATTR
   if (e == cudaSuccess && prepare_xmarch_kernels() != 0) return -1;
   if (e == cudaSuccess && prepare_zstep_tma_kernels() != 0) return -1;
+  if (e == cudaSuccess && prepare_zstep_c_kernels() != 0) return -1;
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -1520,10 +1521,15 @@ bool z_step_takes_tma(const StageArgs& a) {
   return a.zkernel == 1 && a.zmaps && zw == 8 && zstep_tma_supported(a.g);
 }
 
+// the z pass as k_z_step_c: where the solver asks for it and the grid has
+// the levels for its 16 chunks (the chunk count is the kernel's own)
+bool z_step_takes_c(const StageArgs& a) { return a.zkernel == 2 && zstep_c_supported(a.g); }
+
 static void launch_z_step(const StageArgs& a, cudaStream_t st) {
   const Geo& g = a.g;
   const dim3 zgrid(cdiv(g.P, 16), 1, g.nrun);
   const int zw = a.zchunks ? a.zchunks : z_chunks(g, 1);
+  if (z_step_takes_c(a) && launch_z_step_c(a, st)) return;
   if (z_step_takes_tma(a) && launch_z_step_tma(a, st)) return;
   const bool ic = cdiv(g.N3, zw) >= 48;
   if (zw == 16) {

@@ -59,7 +59,7 @@ struct sf_solver {
   int zchunks = 0;               // z chunks per z-solve block (sf_set_z_chunks)
   int xgroups = 0;               // lane groups per x-pass block (sf_set_xpass_groups)
   int xkernel = 1;               // 3D nonlinear x pass: 1 level-marching, 0 slab blocks (sf_set_xpass_kernel)
-  int zkernel = 0;               // z pass: 0 k_z_step, 1 k_z_step_tma (sf_set_z_kernel)
+  int zkernel = 2;               // z pass: 2 k_z_step_c (default), 0 k_z_step, 1 k_z_step_tma (sf_set_z_kernel)
   ZMaps* zmaps = nullptr;        // tensor maps of k_z_step_tma's inputs (null: not supported here)
   int* zerr = nullptr;           // set on the device by a k_z_step_tma wait that ran out
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [linear][parity]
@@ -779,12 +779,13 @@ int sf_profile_names(sf_solver* s, char* buf, size_t len) {
   // the nonlinear 3D x pass runs as k_xmarch where the solver takes it
   const bool march = s->xkernel == 1 && !s->tlm && xmarch_supported(stage_args(s, 0, s->cur, false));
   // and the z pass as k_z_step_tma
-  const bool ztma = z_step_takes_tma(stage_args(s, 0, s->cur, false));
+  const StageArgs a0 = stage_args(s, 0, s->cur, false);
+  const char* zname = z_step_takes_c(a0) ? "k_z_step_c" : (z_step_takes_tma(a0) ? "k_z_step_tma" : "k_z_step");
   for (int k = 0; k < 3; k++)
     for (int i = 0; i < stage_kernel_count(s->g); i++) {
       if (!out.empty()) out += ",";
       const std::string nm = stage_kernel_name(s->g, i);
-      out += (march && nm == "k_xpass") ? std::string("k_xmarch") : (ztma && nm == "k_z_step") ? std::string("k_z_step_tma") : nm;
+      out += (march && nm == "k_xpass") ? std::string("k_xmarch") : nm == "k_z_step" ? std::string(zname) : nm;
     }
   if (out.size() + 1 > len) return fail(SF_EINVAL, "buffer too small");
   std::memcpy(buf, out.c_str(), out.size() + 1);
@@ -861,7 +862,7 @@ int sf_set_xpass_kernel(sf_solver* s, int kind) {
 }
 
 int sf_set_z_kernel(sf_solver* s, int kind) {
-  if (!s || (kind != 0 && kind != 1)) return fail(SF_EINVAL, "kind must be 0 or 1");
+  if (!s || kind < 0 || kind > 2) return fail(SF_EINVAL, "kind must be 0, 1 or 2");
   if (kind != s->zkernel) {
     s->zkernel = kind;
     drop_graphs(s);

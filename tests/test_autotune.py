@@ -20,14 +20,14 @@ def test_search_finds_the_fastest_settings():
     best = {"xkernel": 0, "xy_bands": 6, "xslabs": 2, "z_chunks": 16, "xgroups": 16, "zkernel": 1}
     got, log = A.search(_cost(best), A.space(128, 384))
     assert got == best
-    assert log[0][0] == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0}   # starts from the defaults
+    assert log[0][0] == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 2}   # starts from the defaults
 
 
 def test_search_keeps_the_default_within_the_noise_margin():
     def measure(s):   # every other value is 1% faster: not enough to switch
-        return 0.99 if s != {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0} else 1.0
+        return 0.99 if s != {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 2} else 1.0
     got, _ = A.search(measure, A.space(128, 384))
-    assert got == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 0}
+    assert got == {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 0, "xgroups": 0, "zkernel": 2}
 
 
 def test_each_setting_is_measured_once():
