@@ -21,6 +21,7 @@
 #include "sf_internal.cuh"
 #include "sf_fft.cuh"
 #include "sf_fft2.cuh"
+#include "sf_zstep_c.cuh"
 
 namespace sf {
 
@@ -1063,7 +1064,8 @@ __global__ void __launch_bounds__(kEnsThreads, 2) k_zstep_ens(const StageArgs* _
   const EnsItem it = items[blockIdx.x];
   if (threadIdx.x == 0) sa = args[it.run];
   __syncthreads();
-  if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
+  if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<true>(sa, it.x, 0);
+  else if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
   else z_step_body<8, false>(sa, it.x, 0);
 }
 
@@ -1139,8 +1141,9 @@ __global__ void __launch_bounds__(kEnsThreads, 2) k_ens_stage(const StageArgs* _
         __threadfence();   // this item's r rows, before it counts as done
         atomicAdd(&counters[1 + it.run], 1);
       }
-    } else if (ok) {
-      if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
+    } else if (ok) {   // the member's own z kernel: one lane per complex mode, or one per component
+      if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<true>(sa, it.x, 0);
+      else if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
       else z_step_body<8, false>(sa, it.x, 0);
     }
     __syncthreads();
@@ -1654,7 +1657,9 @@ static int fft_bufstride(int N) {
 size_t ensemble_xpass_smem(int N1, int S) {
   return x_layout(S, N1, N1 / 3, 0, 0, fft_bufstride(N1), kEnsThreads / fft_G(N1), 0, 0).bytes;
 }
-size_t ensemble_zstep_smem(int N3) { return sizeof(float) * ((size_t)N3 * 32 + 3 * 8 * 32); }
+size_t ensemble_zstep_smem(int N3) {
+  return std::max(sizeof(float) * ((size_t)N3 * 32 + 3 * 8 * 32), zc_smem_bytes(N3));
+}
 
 int launch_xpass_ens(const StageArgs* args, const EnsItem* items, int nitems, size_t smem, cudaStream_t st) {
   k_xpass_ens<<<nitems, kEnsThreads, smem, st>>>(args, items);
