@@ -211,8 +211,8 @@ def kernel_bytes(s, name):
 
 
 def pass_of(name):
-    """The pass of the step (the decomposition of SURVEY's per-step model) a
-    kernel belongs to."""
+    """The pass of the step a kernel belongs to: the x-y pass (transforms,
+    products, stencils) or the z pass (implicit solves and projection)."""
     return "z" if name.startswith("k_z") else "xy"
 
 
@@ -341,7 +341,7 @@ def run_reference(args, wl, ws, rank):
 
 
 # ---------------------------------------------------------------------------
-# Newton-Krylov continuation and the learned predictor's
+# Newton-Krylov continuation along Ri (pseudo-arclength) and the learned predictor's
 # study: `--config continuation` and `--config predictor` (2D 256 x 1 x 256,
 # Re 1000, Pr 1, U = tanh z, B = tanh z, dt 0.01, T = 11 as NewtonKrylov.h:113).
 #
@@ -558,7 +558,7 @@ def make_ensemble(wl, device, seed):
 
 
 def ensemble_bytes_per_step(runs):
-    """SURVEY's per-step model summed over the runs: 57 S per 2D run."""
+    """The compulsory per-step traffic summed over the runs: 57 S per 2D run."""
     return sum(57 * n3 * (n1 // 3) * 8 for n1, n3, _ in runs)
 
 
