@@ -687,6 +687,8 @@ def profile_only(args, s):
     (TimeStepAdjoint with the current state at both ends of the step) or net
     (the continuation predictor's forward and gradient passes, batch 16)."""
     import stratiflow_b200 as sf
+    if args.z_kernel >= 0:
+        s.set_z_kernel(args.z_kernel)
     if args.profile_mode == "step":
         s.TimeStep(args.warmup)
         s.synchronize()
@@ -744,6 +746,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="shear3d", choices=sorted(WORKLOADS) + ["continuation", "predictor"])
     ap.add_argument("--no-autotune", action="store_true", help="keep the launchers' default launch settings")
+    ap.add_argument("--z-kernel", type=int, default=-1,
+                    help="--profile-only: the z-pass kernel (sf_set_z_kernel; -1 keeps the solver's)")
     ap.add_argument("--xy-bands", type=int, default=0,
                     help="level bands of the 3D x-y pass (a launch setting; 0: the solver's default)")
     # continuation / predictor studies
