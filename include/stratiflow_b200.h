@@ -188,8 +188,9 @@ int sf_set_xy_bands(sf_solver* s, int bands);
 
 /* Launch tuning of the z solves (no counterpart in the reference): the
  * number of z-chunks one block splits each Thomas system into, 8 or 16 (0:
- * chosen from the grid size). The results depend on it only through
- * rounding (the chunked solve reassociates the recurrence). */
+ * chosen from the grid size), for the z kernels 0 and 1 (sf_set_z_kernel);
+ * the default kernel 2 always splits into 16. The results depend on it only
+ * through rounding (the chunked solve reassociates the recurrence). */
 int sf_set_z_chunks(sf_solver* s, int chunks);
 
 /* Launch tuning of the z pass (no counterpart in the reference): kind 2 (the
