@@ -35,7 +35,7 @@ import time
 from typing import Callable, Dict, List, Tuple
 
 DEFAULTS = {"xkernel": 1, "xslabs": 0, "xy_bands": 1, "z_chunks": 0, "xgroups": 0, "zkernel": 2}
-ORDER = ("xkernel", "xy_bands", "xslabs", "xgroups", "z_chunks", "zkernel")
+ORDER = ("xkernel", "xy_bands", "xslabs", "xgroups", "zkernel", "z_chunks")
 MARGIN = 0.02   # a candidate must be 2% faster to replace the current value
 
 _memory: Dict[str, dict] = {}
@@ -75,6 +75,8 @@ def search(measure: Callable[[dict], float], cand: Dict[str, List[int]], passes:
         for k in ORDER:
             if k not in cand:
                 continue
+            if k == "z_chunks" and cur.get("zkernel") == 2:
+                continue   # the complex-lane z kernel always takes 16 chunks
             for v in cand[k]:
                 if v == cur[k]:
                     continue
