@@ -67,15 +67,18 @@ def test_z_pass_kernels_agree_with_the_z_step(name, nrun, mode, kind):
     _agree(_run(name, 0, nrun, mode), _run(name, kind, nrun, mode), kind)
 
 
-def test_complex_lane_z_pass_with_uneven_chunks():
-    """N3 = 100: 16 chunks of 7 levels, the last of 5 (k_z_step_c's chunk
-    bounds and end tests), against k_z_step."""
-    cfg = dict(CONFIGS["kh2d"], N3=100)
-    CONFIGS["_kh2d_100"] = cfg
+@pytest.mark.parametrize("n3", [100, 36])
+def test_complex_lane_z_pass_with_uneven_chunks(n3):
+    """k_z_step_c's chunk bounds and end tests against k_z_step: N3 = 100
+    gives 16 chunks of 7 levels, the last of 5; N3 = 36 gives 12 chunks of 3
+    levels and 4 empty ones (two warps with no levels, which still take part
+    in the chunk scans)."""
+    name = f"_kh2d_{n3}"
+    CONFIGS[name] = dict(CONFIGS["kh2d"], N3=n3)
     try:
-        _agree(_run("_kh2d_100", 0, 1, "nonlinear"), _run("_kh2d_100", 2, 1, "nonlinear"), 2)
+        _agree(_run(name, 0, 1, "nonlinear"), _run(name, 2, 1, "nonlinear"), 2)
     finally:
-        del CONFIGS["_kh2d_100"]
+        del CONFIGS[name]
 
 
 @pytest.mark.parametrize("kind", [1, 2])
