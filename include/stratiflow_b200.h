@@ -187,10 +187,12 @@ int sf_set_xpass_slabs(sf_solver* s, int slabs);
 int sf_set_xy_bands(sf_solver* s, int bands);
 
 /* Launch tuning of the z solves (no counterpart in the reference): the
- * number of z-chunks one block splits each Thomas system into, 8 or 16 (0:
- * chosen from the grid size), for the z kernels 0 and 1 (sf_set_z_kernel);
- * the default kernel 2 always splits into 16. The results depend on it only
- * through rounding (the chunked solve reassociates the recurrence). */
+ * warps per block of the z solves, 8 or 16 (0: 16 when one block per group
+ * of 16 modes leaves SMs idle, else 8). Each warp takes one z-chunk of every
+ * Thomas system in z kernels 0 and 1 (sf_set_z_kernel) and two in the
+ * default kernel 2, which needs N3 >= 64 for 16 warps (else it takes 8). The
+ * results depend on it only through rounding (the chunked solve
+ * reassociates the recurrence). */
 int sf_set_z_chunks(sf_solver* s, int chunks);
 
 /* Launch tuning of the z pass (no counterpart in the reference): kind 2 (the

@@ -12,7 +12,8 @@ kernels' launch shapes, which change no result (or only its rounding):
             for one slab's inverse transforms in one round)
   xy_bands  level bands of the 3D x-y pass whose y transforms run beside the
             neighbouring bands' x passes (sf_set_xy_bands; 3D only)
-  z_chunks  z-chunks per block of the z solves (sf_set_z_chunks; 0 = the
+  z_chunks  warps per block of the z solves, 8 or 16, each with one z-chunk
+            (k_z_step) or two (k_z_step_c) (sf_set_z_chunks; 0 = the
             launcher's choice from the grid size)
   xkernel   the 3D nonlinear x pass as level-marching warps (1) or slab
             blocks (0) (sf_set_xpass_kernel; 3D only)
@@ -75,8 +76,6 @@ def search(measure: Callable[[dict], float], cand: Dict[str, List[int]], passes:
         for k in ORDER:
             if k not in cand:
                 continue
-            if k == "z_chunks" and cur.get("zkernel") == 2:
-                continue   # the complex-lane z kernel always takes 16 chunks
             for v in cand[k]:
                 if v == cur[k]:
                     continue

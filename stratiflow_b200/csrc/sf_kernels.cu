@@ -1064,7 +1064,7 @@ __global__ void __launch_bounds__(kEnsThreads, 2) k_zstep_ens(const StageArgs* _
   const EnsItem it = items[blockIdx.x];
   if (threadIdx.x == 0) sa = args[it.run];
   __syncthreads();
-  if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<true>(sa, it.x, 0);
+  if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<kCC, true>(sa, it.x, 0);
   else if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
   else z_step_body<8, false>(sa, it.x, 0);
 }
@@ -1142,7 +1142,7 @@ __global__ void __launch_bounds__(kEnsThreads, 2) k_ens_stage(const StageArgs* _
         atomicAdd(&counters[1 + it.run], 1);
       }
     } else if (ok) {   // the member's own z kernel: one lane per complex mode, or one per component
-      if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<true>(sa, it.x, 0);
+      if (sa.zkernel == 2 && zc_fits(sa.g.N3)) z_step_c_body<kCC, true>(sa, it.x, 0);
       else if ((sa.g.N3 + 7) / 8 >= 48) z_step_body<8, true>(sa, it.x, 0);
       else z_step_body<8, false>(sa, it.x, 0);
     }

@@ -10,7 +10,8 @@
 // instructions (FFMA2 / FMUL2 / FADD2: every Thomas coefficient is real, so a
 // complex value times a coefficient is one packed instruction), and each warp
 // carries two z-chunks of the same 16 modes (lanes 0-15 the chunk 2w, lanes
-// 16-31 the chunk 2w+1): a block of 8 warps splits N3 into 16 chunks, so each
+// 16-31 the chunk 2w+1): a block of 8 warps splits N3 into 16 chunks (16
+// warps and 32 chunks for grids too small to fill the GPU), so each
 // serial sweep is half as long and the warp instructions per level are about
 // half of k_z_step's. The arithmetic of every term is k_z_step's, in the same
 // order; the chunked scan over 16 chunks instead of 8 reassociates the
@@ -23,8 +24,8 @@
 
 namespace sf {
 
-constexpr int kCW = 8;         // warps per block
-constexpr int kCC = 2 * kCW;   // z-chunks per block, two per warp
+constexpr int kCC = 16;        // z-chunks per block (two per warp) of the default block of 8 warps;
+                               // grids too small to fill the GPU take 32 (16 warps)
 constexpr int kCU = 2;         // levels of every input loaded ahead in the first sweep
 constexpr int kCI = 8;         // levels of inverse pivots loaded ahead in the later sweeps
 constexpr int kCP = 4;         // levels of the fields loaded ahead in the projection's last sweep
@@ -37,22 +38,24 @@ __device__ __forceinline__ float2 czik(float k, float2 z) { return make_float2(-
 
 struct ZcShared {
   float2* D;     // [N3][16]: be_j, then D_j
-  float* A;      // [kCC][16]
-  float2* B;     // [kCC][16]
-  float2* In;    // [kCC][16]
+  float* A;      // [CC][16]
+  float2* B;     // [CC][16]
+  float2* In;    // [CC][16]
 };
+template <int CC>
 __device__ __forceinline__ ZcShared zc_shared(int N3) {
   extern __shared__ __align__(16) float zcsm[];
   ZcShared s;
   s.D = reinterpret_cast<float2*>(zcsm);
   s.B = s.D + (size_t)N3 * 16;
-  s.In = s.B + kCC * 16;
-  s.A = reinterpret_cast<float*>(s.In + kCC * 16);
+  s.In = s.B + CC * 16;
+  s.A = reinterpret_cast<float*>(s.In + CC * 16);
   return s;
 }
 
-// the scan of the chunks' affine maps v -> A v + B over the 16 chunks of a
+// the scan of the chunks' affine maps v -> A v + B over the CC chunks of a
 // block, upward (D) or downward (x), one lane per mode of warp 0
+template <int CC>
 __device__ __forceinline__ float2 zc_scan(const ZcShared& sh, int ch, int ml, int w, int lane, float A, float2 B,
                                           bool up) {
   sh.A[ch * 16 + ml] = A;
@@ -60,8 +63,8 @@ __device__ __forceinline__ float2 zc_scan(const ZcShared& sh, int ch, int ml, in
   __syncthreads();
   if (w == 0 && lane < 16) {
     float2 v = cz();
-    for (int i = 0; i < kCC; i++) {
-      const int k = up ? i : kCC - 1 - i;
+    for (int i = 0; i < CC; i++) {
+      const int k = up ? i : CC - 1 - i;
       sh.In[k * 16 + lane] = v;
       v = cfma(sh.A[k * 16 + lane], v, sh.B[k * 16 + lane]);
     }
@@ -113,7 +116,7 @@ __device__ __forceinline__ ZcMap zc_sweep2(const ZcShared& sh, int js, int je, i
 }
 
 // the CN solve of field f of family FAM (0: u1, u2; 1: u3, Dirichlet; 2: b)
-template <int FAM, bool IC>
+template <int CC, int FAM, bool IC>
 __device__ __forceinline__ void zc_cn(const StageArgs& a, const int f, const int bx, const int bz) {
   const Geo g = a.g;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -123,9 +126,9 @@ __device__ __forceinline__ void zc_cn(const StageArgs& a, const int f, const int
   const int m = act ? m0 : 0;
   const int run = bz;
   const int N3 = g.N3, Pp = g.Pp;
-  const int chunk = (N3 + kCC - 1) / kCC;
+  const int chunk = (N3 + CC - 1) / CC;
   const int js = min(N3, ch * chunk), je = min(N3, js + chunk);
-  const ZcShared sh = zc_shared(N3);
+  const ZcShared sh = zc_shared<CC>(N3);
   const int q = m / g.K1, j1 = m - q * g.K1;
   const float kxv = a.kx[j1], kyv = a.ky[q];
   const float d1 = -(kxv * kxv), d2 = -(kyv * kyv);
@@ -236,11 +239,11 @@ __device__ __forceinline__ void zc_cn(const StageArgs& a, const int f, const int
   };
   if (interior) sweep1(std::true_type{});
   else sweep1(std::false_type{});
-  const float2 Din = zc_scan(sh, ch, ml, w, lane, A, B, true);
+  const float2 Din = zc_scan<CC>(sh, ch, ml, w, lane, A, B, true);
   auto Cof = [&](int j, float bij) { return fc[j] * bij; };
   const ZcMap bk = interior ? zc_sweep2<true>(sh, js, je, ml, Din, fa, iden, Pp, Cof)
                             : zc_sweep2<false>(sh, js, je, ml, Din, fa, iden, Pp, Cof);
-  float2 x = zc_scan(sh, ch, ml, w, lane, bk.A, bk.B, false);
+  float2 x = zc_scan<CC>(sh, ch, ml, w, lane, bk.A, bk.B, false);
   // ---- backward: x_j = D_j - C_j x_{j+1} ----
   auto sweep3 = [&](auto tag) {
     constexpr bool IN = decltype(tag)::value;
@@ -263,6 +266,7 @@ __device__ __forceinline__ void zc_cn(const StageArgs& a, const int f, const int
 // RemoveDivergence on the new velocities: the divergence and the Laplacian
 // factors upward, q downward, then u -= grad q and p += pm q (k_z_step's
 // projection, one lane per complex mode)
+template <int CC>
 __device__ __forceinline__ void zc_proj(const StageArgs& a, const int bx, const int bz) {
   const Geo g = a.g;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -272,9 +276,9 @@ __device__ __forceinline__ void zc_proj(const StageArgs& a, const int bx, const 
   const int m = act ? m0 : 0;
   const int run = bz;
   const int N3 = g.N3, Pp = g.Pp;
-  const int chunk = (N3 + kCC - 1) / kCC;
+  const int chunk = (N3 + CC - 1) / CC;
   const int js = min(N3, ch * chunk), je = min(N3, js + chunk);
-  const ZcShared sh = zc_shared(N3);
+  const ZcShared sh = zc_shared<CC>(N3);
   const int q = m / g.K1, j1 = m - q * g.K1;
   const float kxv = a.kx[j1], kyv = g.dim3 ? a.ky[q] : 0.f;
   const size_t S1 = (size_t)Pp;
@@ -326,14 +330,14 @@ __device__ __forceinline__ void zc_proj(const StageArgs& a, const int bx, const 
       w0 = w1;
     }
   }
-  const float2 Din = zc_scan(sh, ch, ml, w, lane, A, B, true);
+  const float2 Din = zc_scan<CC>(sh, ch, ml, w, lane, A, B, true);
   auto Cof = [&](int j, float bij) {
     float Cj = c_[j] * bij;
     if (m == 0 && j == 1) Cj = 0.f;   // (0,0) mode: row 1 pinned (IMEXRK.h:68-74)
     return Cj;
   };
   const ZcMap bk = zc_sweep2<false>(sh, js, je, ml, Din, a_, iden, Pp, Cof);
-  float2 qn = zc_scan(sh, ch, ml, w, lane, bk.A, bk.B, false);   // q at level je
+  float2 qn = zc_scan<CC>(sh, ch, ml, w, lane, bk.A, bk.B, false);   // q at level je
   // ---- backward, pass 2: q_j, projection, p; every row of u1, u2, u3, p is
   // written once, by the step of one level, so the loads of a batch may all
   // go ahead of its stores ----
@@ -372,23 +376,25 @@ __device__ __forceinline__ void zc_proj(const StageArgs& a, const int bx, const 
 // bz: the CN solves of every field, then RemoveDivergence on the new
 // velocities, which the block has just written (visible to it after the
 // barrier). Needs N3 >= 32 and zc_smem_bytes(N3) of dynamic shared memory.
-template <bool IC>
+template <int CC, bool IC>
 __device__ __forceinline__ void z_step_c_body(const StageArgs& a, const int bx, const int bz) {
   if (a.g.dim3) {
-    zc_cn<0, IC>(a, 0, bx, bz);
-    zc_cn<0, IC>(a, 1, bx, bz);
+    zc_cn<CC, 0, IC>(a, 0, bx, bz);
+    zc_cn<CC, 0, IC>(a, 1, bx, bz);
   } else {
-    zc_cn<0, IC>(a, 0, bx, bz);
+    zc_cn<CC, 0, IC>(a, 0, bx, bz);
   }
-  zc_cn<1, IC>(a, 2, bx, bz);
-  zc_cn<2, IC>(a, 3, bx, bz);
+  zc_cn<CC, 1, IC>(a, 2, bx, bz);
+  zc_cn<CC, 2, IC>(a, 3, bx, bz);
   __syncthreads();
-  zc_proj(a, bx, bz);
+  zc_proj<CC>(a, bx, bz);
 }
 
+template <int CC = kCC>
 __host__ __device__ inline size_t zc_smem_bytes(int N3) {
-  return sizeof(float2) * ((size_t)N3 * 16 + 2 * kCC * 16) + sizeof(float) * kCC * 16;
+  return sizeof(float2) * ((size_t)N3 * 16 + 2 * CC * 16) + sizeof(float) * CC * 16;
 }
-__host__ __device__ inline bool zc_fits(int N3) { return N3 >= 2 * kCC; }
+template <int CC = kCC>
+__host__ __device__ inline bool zc_fits(int N3) { return N3 >= 2 * CC; }
 
 }  // namespace sf

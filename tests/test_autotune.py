@@ -87,18 +87,3 @@ def test_tune_applies_and_caches_the_plan(tmp_path, monkeypatch):
     again, log2 = A.tune(s2, steps=1)
     assert again == best and log2 == [] and s2.applied == best   # from the cache
 
-
-def test_z_chunks_are_not_timed_under_the_complex_lane_z_kernel():
-    """The complex-lane z kernel (zkernel 2) always splits into 16 chunks, so
-    while it is the choice no z_chunks candidate is measured; once another z
-    kernel wins, the z_chunks candidates are."""
-    seen = []
-
-    def measure(s):
-        seen.append(dict(s))
-        return 1.0   # nothing is faster: the defaults stay
-    A.search(measure, A.space(128, 384))
-    assert all(s["z_chunks"] == 0 for s in seen if s["zkernel"] == 2)
-    best = {"xkernel": 1, "xy_bands": 1, "xslabs": 0, "z_chunks": 8, "xgroups": 0, "zkernel": 0}
-    got, _ = A.search(_cost(best), A.space(128, 384))
-    assert got == best

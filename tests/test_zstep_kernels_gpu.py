@@ -3,8 +3,9 @@ k_z_step_tma (kind 1: each warp brings its first Thomas sweeps' inputs into
 a shared-memory ring with tensor-map copies, the sweeps' intermediates live
 in tensor memory), the same chunked solve with the same terms in the same
 order; and k_z_step_c (kind 2: one lane per complex mode in packed FP32, two
-z-chunks per warp, 16 chunks per block), the same terms, with the
-recurrences split into 16 chunks instead of 8. The states agree to the bits
+z-chunks per warp: 16 chunks in blocks of 8 warps, 32 in blocks of 16
+warps on the grids here that leave SMs idle), the same terms, with the
+recurrences split into more chunks. The states agree to the bits
 the compilations round differently: for kind 1, 1e-6 relative L2 per field
 after 4 steps (5e-5 for p); for kind 2, whose chunking reassociates every
 recurrence, to the parity tests' bound against the FP64 oracle (1e-5 per
@@ -23,7 +24,8 @@ pytestmark = pytest.mark.gpu
 def _run(name, kind, nrun, mode, steps=4):
     cfg = CONFIGS[name]
     s = gpu_solver(cfg, nrun=nrun)
-    s.set_z_chunks(8)
+    if kind in (0, 1):
+        s.set_z_chunks(8)   # the tensor-map kernel takes 8 chunks; the baseline the same
     s.set_z_kernel(kind)
     for r in range(nrun):
         s.set_state(r, make_ic(cfg, seed=800 + r, amp=5e-2 if r == 0 else 1e-3))
@@ -96,7 +98,8 @@ def test_z_pass_kernels_agree_in_the_adjoint_step(kind):
         below = kept([make_ic(cfg, seed=851 + r, amp=5e-2) for r in range(2)])
         above = kept([make_ic(cfg, seed=861 + r, amp=5e-2) for r in range(2)])
         s = gpu_solver(cfg, nrun=2)
-        s.set_z_chunks(8)
+        if kind in (0, 1):
+            s.set_z_chunks(8)
         s.set_z_kernel(kind)
         for r in range(2):
             s.set_state(r, make_ic(cfg, seed=871 + r, amp=1e-3))
@@ -108,3 +111,26 @@ def test_z_pass_kernels_agree_in_the_adjoint_step(kind):
         s.close()
         return out
     _agree(run(0), run(kind), kind)
+
+
+@pytest.mark.parametrize("warps", [8, 16])
+def test_complex_lane_z_pass_block_sizes(warps):
+    """k_z_step_c with 8 warps (16 chunks) and 16 warps (32 chunks) per block,
+    forced through sf_set_z_chunks, on the 3D grid 64 x 32 x 64 with two
+    runs, against k_z_step."""
+    cfg = CONFIGS["shear3d_small"]
+
+    def run(kind, z):
+        s = gpu_solver(cfg, nrun=2)
+        s.set_z_kernel(kind)
+        s.set_z_chunks(z)
+        for r in range(2):
+            s.set_state(r, make_ic(cfg, seed=880 + r, amp=5e-2))
+        s.Prepare()
+        s.TimeStep(4)
+        s.synchronize()
+        out = s.get_state_kept()
+        s.close()
+        return out
+    _agree(run(0, 8), run(2, warps), 2)
+
