@@ -417,8 +417,9 @@ class IMEXRK:
         _check(load_library().sf_set_z_kernel(self._h, int(kind)))
 
     def set_z_chunks(self, chunks):
-        """z chunks per block of the z solves (0: automatic, 8 or 16); a
-        launch setting (the results change only by rounding)."""
+        """Warps per block of the z solves (0: automatic, 8 or 16), each with
+        one z-chunk (k_z_step) or two (k_z_step_c); a launch setting (the
+        results change only by rounding)."""
         _check(load_library().sf_set_z_chunks(self._h, int(chunks)))
 
     def set_tangent(self, nbase):
